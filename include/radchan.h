@@ -1,0 +1,288 @@
+/*
+ * radchan.h -- C ABI of the B200 (sm_100a) narrow-band correlated-k OERM
+ * Monte Carlo radiative-transfer solver.
+ *
+ * This library is a drop-in for the GPU radiation solver of RadChan
+ * (src/montecarlo).  The reference exposes two Fortran-callable symbols,
+ * declared here with the same names, arguments and array layouts:
+ *
+ *   mc_gpu_      (src/montecarlo/mc_gpu_noint.cu:660)  -- launch, returns
+ *                without waiting for the device;
+ *   get_results_ (src/montecarlo/mc_gpu_noint.cu:876)  -- wait, fill Q and
+ *                its Monte Carlo standard deviation.
+ *
+ * The reference configures everything at compile time (src/param/param.h,
+ * src/param/NarrowBand.h) and reads its spectral tables from
+ * properties/*.txt on every call (src/montecarlo/read_tables.cpp:21-96).
+ * Here the same parameter set is a runtime struct (rc_params), which can be
+ * filled from an existing param.h / NarrowBand.h pair, and the tables are
+ * uploaded once and stay resident on the device.
+ *
+ * Conventions
+ *  - Every rc_* function returns an int status: RC_OK (0) or a negative
+ *    RC_E* code; rc_last_error() returns the message of the last failure
+ *    on that context (or of the last context-free call when ctx is NULL).
+ *  - All buffers passed in belong to the caller; the library copies them.
+ *  - Temperature fields are float, Fortran order (i fastest), with one
+ *    ghost layer: T(0:imax+1, 0:jmax+1, 0:kmax+1), index
+ *    i + (imax+2)*(j + (jmax+2)*k)   (param.h:132 idx_T).
+ *  - Result arrays are float Q(0:imax+1, 0:jmax+1, 0:kloc+1) with
+ *    kloc = kmax/p_col (param.h:138 idx_F, mc_gpu_noint.cu:876): interior
+ *    cells receive the radiative source (W/m^3 with SI tables), i = 0 and
+ *    i = imax+1 receive the net wall flux (W/m^2) of adiabatic x-walls when
+ *    calcwalls = 1, else 0.  Other ghost entries are left untouched.
+ *  - One context per host thread; a context is not re-entrant.  The
+ *    library never calls cudaDeviceReset.
+ */
+#ifndef RADCHAN_H_
+#define RADCHAN_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define RC_MAX_LEVELS 9   /* param.h:24 grid_num is at most 9 */
+
+/* status codes */
+#define RC_OK            0
+#define RC_E_INVALID    -1   /* bad argument or parameter combination */
+#define RC_E_CUDA       -2   /* a CUDA runtime call failed */
+#define RC_E_NOMEM      -3   /* device or host allocation failed / budget */
+#define RC_E_IO         -4   /* table file missing or malformed */
+#define RC_E_STATE      -5   /* call out of order (e.g. collect w/o solve) */
+#define RC_E_RANGE      -6   /* T outside the table range or not finite */
+#define RC_E_BUSY       -7   /* no free slot / queue full */
+#define RC_E_NOTFOUND   -8
+
+/* wall indices: west (x=0), east (x=Lx), south (y=0), north (y=Ly),
+ * bottom (z=0), top (z=Lz) -- the order of param.h:68-100 */
+enum { RC_WEST = 0, RC_EAST, RC_SOUTH, RC_NORTH, RC_BOT, RC_TOP };
+
+/* boundary types, param.h:90-94 */
+#define RC_BD_PERIODIC 1
+#define RC_BD_BLACK    2
+#define RC_BD_SPECULAR 3
+#define RC_BD_ADIABLK  4   /* black wall at the temperature of the first cell */
+#define RC_BD_LOST     5
+
+/* Runtime image of src/param/param.h + NarrowBand.h. */
+typedef struct rc_params {
+    int imax, jmax, kmax;               /* param.h:10-12 */
+    float Lx, Ly, Lz;                   /* param.h:13-15 (m) */
+    double fact_mesh;                   /* param.h:16 parabolic x stretching */
+    int nVar;                           /* param.h:18 replicates */
+    int photmax;                        /* param.h:19 bundles per cell and replicate */
+    double chanHeight;                  /* param.h:20 scales k and kP on load */
+    int grid_num;                       /* param.h:24 */
+    int maxi[RC_MAX_LEVELS], maxj[RC_MAX_LEVELS], maxk[RC_MAX_LEVELS]; /* :27-29 */
+    int maxs[RC_MAX_LEVELS];            /* param.h:31-49 step budget per level */
+    int num_gpu, p_col;                 /* param.h:8-9 (num_gpu must be 1) */
+    int num_streams, blockdim, nblocks; /* param.h:52-54, accepted as hints */
+    int srt;                            /* param.h:57 band-sorted bundle order */
+    int grey;                           /* param.h:59 grey gas (NarrowBand.h:213-221) */
+    int calcwalls;                      /* param.h:61 wall-flux kernel */
+    int random;                         /* param.h:63 (Sobol in the reference; here
+                                           Philox counters are always used) */
+    int floatpoint;                     /* param.h:65 1 -> full FP64 kernels */
+    float eps[6];                       /* param.h:68-73 wall emissivities */
+    float Tw[6];                        /* param.h:75-80 wall temperatures (K) */
+    int adiabw, adiabe;                 /* param.h:82-83 */
+    double stefan;                      /* param.h:85 */
+    float toll, tollS;                  /* param.h:86-87 transmissivity cutoffs */
+    int bd[6];                          /* param.h:95-100 */
+    /* grey-gas constants, NarrowBand.h:214-219 */
+    int grey_nT, grey_nB;
+    float abscoeff, Tmins, wvmax;
+    /* narrow-band table dimensions, NarrowBand.h:189-191 */
+    int nT, nQ, nB;
+    /* Philox key of the bundle streams */
+    uint64_t seed;
+} rc_params;
+
+/* Spectral tables in the reference's layout (read_tables.cpp:21-96).
+ * kq and kP are given unscaled; the library multiplies them by
+ * chanHeight as readT does (read_tables.cpp:30,56). */
+typedef struct rc_tables {
+    int nT, nB, nQ;
+    const float *Tnb;    /* [nT] table temperatures, uniformly spaced (K) */
+    const float *kP;     /* [nT] Planck-mean absorption coefficient */
+    const float *wvl;    /* [nB] band left edge (cm^-1) */
+    const float *wvr;    /* [nB] band right edge (cm^-1) */
+    const float *wvc;    /* [nB] band centre (cm^-1) */
+    const float *kavg;   /* [nB] band-mean k used as the sort key (srt) */
+    const float *kq;     /* [nB][nT][nQ] k at each g point */
+    const float *prob;   /* [nT][nB] cumulative band probability */
+    const float *probg;  /* [nT][nB][nQ] cumulative g probability */
+    const float *wq;     /* [nQ] g-quadrature weights */
+} rc_tables;
+
+/* Seeded synthetic correlated-k table recipe: k_{b,g}(T) =
+ * k0_b exp(kexp xi_g) (T/1000)^{n_b}, log10 k0_b ~ U[logk_lo, logk_hi],
+ * n_b ~ U[-nexp, nexp], xi_g the nQ-point Gauss-Legendre nodes on [-1,1],
+ * band centres ~ U[nu_lo, nu_hi] sorted, nT temperatures on [T_lo, T_hi]. */
+typedef struct rc_synth_spec {
+    int nB, nQ, nT;
+    double T_lo, T_hi;
+    double nu_lo, nu_hi;
+    double logk_lo, logk_hi;
+    double nexp, kexp;
+    uint64_t seed;
+} rc_synth_spec;
+
+/* Host-owned table set (returned by the builders below). */
+typedef struct rc_table_set rc_table_set;
+
+typedef struct rc_ctx rc_ctx;
+typedef int32_t rc_ticket;
+
+/* ---------------- parameters ---------------- */
+
+/* Fill with the reference's defaults (param.h, NarrowBand.h as shipped). */
+int rc_params_default(rc_params *p);
+/* Parse an existing param.h and (optional) NarrowBand.h: #define lines,
+ * the maxi/maxj/maxk/maxs initialisers and their #if grid_num branches. */
+int rc_params_from_headers(const char *param_h, const char *narrowband_h, rc_params *p);
+/* Check a parameter set; returns RC_E_INVALID with a message on failure. */
+int rc_params_validate(const rc_params *p, char *msg, size_t msglen);
+
+/* ---------------- tables ---------------- */
+
+int rc_tables_synthetic(const rc_synth_spec *spec, rc_table_set **out);
+/* Read properties/planck-mean.txt, NarrBand%d.txt and prob_new2.txt from
+ * dir in the formats of nbcorrk/write_tables.cpp:23-107. */
+int rc_tables_read_dir(const char *dir, int nT, int nB, int nQ, rc_table_set **out);
+int rc_tables_write_dir(const rc_table_set *ts, const char *dir);
+/* Borrowed view of a table set (valid until rc_tables_free). */
+int rc_tables_view(const rc_table_set *ts, rc_tables *view);
+void rc_tables_free(rc_table_set *ts);
+
+/* ---------------- solver context ---------------- */
+
+int rc_create(const rc_params *p, int device, rc_ctx **out);
+int rc_set_tables(rc_ctx *ctx, const rc_tables *t);
+/* Copy T (host, whole field incl. ghosts) and launch; returns at once. */
+int rc_solve_async(rc_ctx *ctx, const float *T, int zstart, rc_ticket *ticket);
+/* Same with T already in device memory (same layout). */
+int rc_solve_device_async(rc_ctx *ctx, const float *T_dev, int zstart, rc_ticket *ticket);
+/* Wait for a ticket and fill the caller's arrays.  Q and sigma use the
+ * Fortran result layout above (either may be NULL).  The optional double
+ * outputs use compact layouts: q64/var64 [kloc][jmax][imax] (per-cell mean
+ * and variance of the mean), qw64/vw64 [2][kloc][jmax] (west, east). */
+int rc_collect(rc_ctx *ctx, rc_ticket ticket, float *Q, float *sigma,
+               double *q64, double *var64, double *qw64, double *vw64);
+/* Device-side results of the last collected/finished ticket (no copy):
+ * pointers to the compact double arrays described above. */
+int rc_device_results(rc_ctx *ctx, rc_ticket ticket, const double **q64,
+                      const double **var64, const double **qw64, const double **vw64);
+/* Per-solve diagnostics of a finished ticket. */
+typedef struct rc_solve_info {
+    float Tmax;            /* max of interior T and x-wall face averages */
+    float kappamax;        /* Planck-mean k at Tmax */
+    float Ibmax_fluid;     /* energy per fluid bundle */
+    int   table_row;       /* table row nearest Tmax (mc_gpu_noint.cu:1110) */
+    int   status;          /* bit 0: T outside table range, bit 1: non-finite T */
+    double bundles;        /* bundles traced */
+    double steps;          /* ray-cell steps */
+    float ms_device;       /* device time of the march kernel */
+    float ms_solve;        /* device time of the whole solve (copy-in .. tally) */
+} rc_solve_info;
+int rc_solve_info_get(rc_ctx *ctx, rc_ticket ticket, rc_solve_info *info);
+/* Launch knobs of the march kernel; values <= 0 (sort_bands < 0) keep the
+ * current setting.  rays_per_thread: bundles per work item (power of two
+ * <= 64; it fixes the FP64 summation grouping, results differ only by
+ * rounding); block_threads: 128 or 256; sort_bands: band-sorted bundle
+ * order within a warp's pool (srt); occupancy: resident 256-thread blocks
+ * per SM the register budget must allow (2, 3 or 4).  None of them changes
+ * which bundles are traced. */
+int rc_set_launch(rc_ctx *ctx, int rays_per_thread, int block_threads, int sort_bands, int occupancy);
+int rc_get_launch(rc_ctx *ctx, int *rays_per_thread, int *block_threads, int *sort_bands, int *occupancy);
+/* Try launch configurations on T (host) with a reduced bundle count
+ * (pilot_photmax) and keep the fastest; writes the chosen knobs. */
+int rc_autotune(rc_ctx *ctx, const float *T, int zstart, int pilot_photmax,
+                int *rays_per_thread, int *block_threads, int *occupancy);
+int rc_destroy(rc_ctx *ctx);
+int rc_last_error(const rc_ctx *ctx, char *buf, size_t len);
+/* Grid faces/centres of level `level` as built by the library
+ * (definitions.h:68-136); any pointer may be NULL. */
+int rc_grid_level(const rc_params *p, int level, float *xu, float *yu, float *zu,
+                  float *x, float *y, float *z);
+
+/* ---------------- bundle traces (parity checks) ---------------- */
+
+/* One traced bundle: kind 0 = fluid cell (i,j,k), 1 = west wall (j,k),
+ * 2 = east wall (j,k); v replicate; h bundle index. */
+typedef struct rc_bundle_id { int kind, i, j, k, v, h; } rc_bundle_id;
+typedef struct rc_trace_rec {
+    int nb, g;             /* sampled band and g point */
+    int nsteps;            /* ray-cell steps taken */
+    int end_level;         /* multigrid level at the end */
+    float sx, sy, sz;      /* emission direction */
+    float tra;             /* final transmissivity */
+    double De;             /* the bundle's tally contribution */
+} rc_trace_rec;
+/* Trace bundles of the ticket's problem; cells[n*max_cells*4] receives
+ * (level, ic, jc, kc) of the first max_cells steps of each bundle. */
+int rc_trace(rc_ctx *ctx, rc_ticket ticket, int n, const rc_bundle_id *ids,
+             rc_trace_rec *out, int max_cells, int *cells);
+
+/* ---------------- batched solves ---------------- */
+
+typedef struct rc_batch rc_batch;
+/* A batch runs many contexts' solves (uneven grids, tables, photmax) in
+ * one persistent work-queue launch; with use_graph the whole sequence
+ * (copies + kernels) is captured once and replayed. */
+int rc_batch_create(int device, int use_graph, rc_batch **out);
+int rc_batch_add(rc_batch *b, rc_ctx *ctx, const float *T_host, int zstart);
+int rc_batch_run(rc_batch *b);          /* enqueue; returns at once */
+int rc_batch_wait(rc_batch *b, float *ms_device);
+int rc_batch_collect(rc_batch *b, int index, float *Q, float *sigma,
+                     double *q64, double *var64, double *qw64, double *vw64);
+int rc_batch_destroy(rc_batch *b);
+
+/* ---------------- serving ---------------- */
+
+typedef struct rc_server rc_server;
+typedef struct rc_request {
+    const rc_params *params;     /* grid, photmax (0 -> from tolerance), ... */
+    int table_set;               /* id from rc_server_add_tables */
+    const float *T;              /* host field, copied at submit */
+    int zstart;
+    float tolerance;             /* target rel. std of max|Q| (0: use photmax) */
+} rc_request;
+typedef struct rc_result_info {
+    double t_submit, t_admit, t_done;   /* seconds, server clock */
+    int photmax;                        /* bundles per cell used */
+    float rel_std_maxq;                 /* achieved rel. std at argmax |Q| */
+    int status;
+} rc_result_info;
+int rc_server_create(int device, double hbm_budget_bytes, int max_inflight, rc_server **out);
+int rc_server_add_tables(rc_server *s, const rc_tables *t, int *table_set);
+int rc_server_submit(rc_server *s, const rc_request *req, int64_t *id);
+/* Wait for a request; Q/sigma in the Fortran result layout (may be NULL). */
+int rc_server_wait(rc_server *s, int64_t id, float *Q, float *sigma, rc_result_info *info);
+int rc_server_stats(rc_server *s, double *solves, double *busy_s, double *hbm_in_use);
+int rc_server_destroy(rc_server *s);
+
+/* ---------------- reference-compatible entry points ---------------- */
+
+/* Configure the process-wide context used by mc_gpu_/get_results_.
+ * tables may be NULL in grey mode.  Without this call the first mc_gpu_
+ * reads RADCHAN_PARAM_H / RADCHAN_NARROWBAND_H (paths of the reference's
+ * headers) and RADCHAN_PROPERTIES (directory of the table files, default
+ * ./properties). */
+int rc_legacy_configure(const rc_params *p, const rc_tables *tables);
+int rc_legacy_release(void);
+/* mc_gpu_noint.cu:660 -- T is the whole (0:imax+1,0:jmax+1,0:kmax+1) field,
+ * zstart the 1-based first z index of this slab; returns before the device
+ * finishes.  Errors are printed and kept for rc_last_error(NULL, ...). */
+void mc_gpu_(float *T, int *zstart, int *rank);
+/* mc_gpu_noint.cu:876 -- waits, then fills Q and sigma (Fortran layout). */
+void get_results_(float *Q, float *sigma, int *rank);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* RADCHAN_H_ */

@@ -1,0 +1,266 @@
+"""Python mirror of the solver interface (ctypes over libradchan.so).
+
+Mirrors the reference's operator interface for this path: a parameter set
+equivalent to src/param/param.h + NarrowBand.h, spectral tables in the
+layout of src/montecarlo/read_tables.cpp, and a solve that takes the whole
+temperature field T(0:imax+1, 0:jmax+1, 0:kmax+1) and returns the radiative
+source Q and its Monte Carlo standard deviation in the layout of
+get_results_ (src/montecarlo/mc_gpu_noint.cu:876).
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _lib as L
+
+
+def default_params() -> L.RcParams:
+    p = L.RcParams()
+    L.check(L.lib().rc_params_default(C.byref(p)))
+    return p
+
+
+def params_from_headers(param_h: str, narrowband_h: str | None = None) -> L.RcParams:
+    p = L.RcParams()
+    L.check(L.lib().rc_params_from_headers(param_h.encode(), narrowband_h.encode() if narrowband_h else None,
+                                           C.byref(p)))
+    return p
+
+
+def validate(p: L.RcParams) -> str:
+    buf = C.create_string_buffer(512)
+    rc = L.lib().rc_params_validate(C.byref(p), buf, 512)
+    return "" if rc == 0 else buf.value.decode()
+
+
+def set_levels(p: L.RcParams, levels, maxs):
+    """levels: list of (im, jm, km), finest first; maxs: step budgets."""
+    p.grid_num = len(levels)
+    for l, (a, b, c) in enumerate(levels):
+        p.maxi[l], p.maxj[l], p.maxk[l] = a, b, c
+        p.maxs[l] = maxs[l]
+    return p
+
+
+def copy_params(p: L.RcParams) -> L.RcParams:
+    q = L.RcParams()
+    C.memmove(C.byref(q), C.byref(p), C.sizeof(L.RcParams))
+    return q
+
+
+def grid_level(p: L.RcParams, level: int = 0):
+    im, jm, km = p.maxi[level], p.maxj[level], p.maxk[level]
+    arrs = {n: np.zeros(s, np.float32) for n, s in
+            (("xu", im + 1), ("yu", jm + 1), ("zu", km + 1), ("x", im + 2), ("y", jm + 2), ("z", km + 2))}
+    fp = lambda a: a.ctypes.data_as(C.POINTER(C.c_float))
+    L.check(L.lib().rc_grid_level(C.byref(p), level, fp(arrs["xu"]), fp(arrs["yu"]), fp(arrs["zu"]),
+                                  fp(arrs["x"]), fp(arrs["y"]), fp(arrs["z"])))
+    return arrs
+
+
+class TableSet:
+    """Host-owned spectral table set (correlated-k tables)."""
+
+    def __init__(self, handle):
+        self.h = C.c_void_p(handle) if not isinstance(handle, C.c_void_p) else handle
+        self.view = L.RcTables()
+        L.check(L.lib().rc_tables_view(self.h, C.byref(self.view)))
+
+    @classmethod
+    def synthetic(cls, nB=100, nQ=8, nT=64, T_lo=300.0, T_hi=2000.0, nu_lo=500.0, nu_hi=10000.0,
+                  logk_lo=-3.0, logk_hi=2.0, nexp=1.0, kexp=1.5, seed=20240601):
+        s = L.RcSynthSpec(nB, nQ, nT, T_lo, T_hi, nu_lo, nu_hi, logk_lo, logk_hi, nexp, kexp, seed)
+        h = C.c_void_p()
+        L.check(L.lib().rc_tables_synthetic(C.byref(s), C.byref(h)))
+        return cls(h)
+
+    @classmethod
+    def read_dir(cls, path, nT, nB, nQ):
+        h = C.c_void_p()
+        L.check(L.lib().rc_tables_read_dir(str(path).encode(), nT, nB, nQ, C.byref(h)))
+        return cls(h)
+
+    def write_dir(self, path):
+        L.check(L.lib().rc_tables_write_dir(self.h, str(path).encode()))
+
+    def arrays(self):
+        v = self.view
+        nT, nB, nQ = v.nT, v.nB, v.nQ
+        f = lambda ptr, n: np.ctypeslib.as_array(ptr, shape=(n,)).copy()
+        return dict(nT=nT, nB=nB, nQ=nQ, Tnb=f(v.Tnb, nT), kP=f(v.kP, nT), wvl=f(v.wvl, nB), wvr=f(v.wvr, nB),
+                    wvc=f(v.wvc, nB), kavg=f(v.kavg, nB), kq=f(v.kq, nB * nT * nQ).reshape(nB, nT, nQ),
+                    prob=f(v.prob, nT * nB).reshape(nT, nB), probg=f(v.probg, nT * nB * nQ).reshape(nT, nB, nQ),
+                    wq=f(v.wq, nQ))
+
+    def __del__(self):
+        try:
+            if self.h:
+                L.lib().rc_tables_free(self.h)
+                self.h = None
+        except Exception:
+            pass
+
+
+def field_shape(p):
+    """numpy shape of the temperature field: (kmax+2, jmax+2, imax+2), i fastest."""
+    return (p.kmax + 2, p.jmax + 2, p.imax + 2)
+
+
+def result_shape(p):
+    return (p.kmax // p.p_col + 2, p.jmax + 2, p.imax + 2)
+
+
+@dataclass
+class Result:
+    Q: np.ndarray          # Fortran-layout float result (kloc+2, jmax+2, imax+2)
+    sigma: np.ndarray
+    q64: np.ndarray        # [kloc, jmax, imax] per-cell mean (FP64)
+    var64: np.ndarray      # variance of the mean
+    qw64: np.ndarray       # [2, kloc, jmax] wall fluxes (west, east)
+    vw64: np.ndarray
+
+
+class Solver:
+    """One solver context on one GPU (rc_create .. rc_destroy)."""
+
+    def __init__(self, params: L.RcParams, tables: TableSet | None = None, device: int = 0):
+        self.p = copy_params(params)
+        self.ctx = C.c_void_p()
+        L.check(L.lib().rc_create(C.byref(self.p), device, C.byref(self.ctx)))
+        self.tables = tables
+        if tables is not None and not self.p.grey:
+            L.check(L.lib().rc_set_tables(self.ctx, C.byref(tables.view)), self.ctx)
+
+    def set_launch(self, rays_per_thread=0, block_threads=0, sort_bands=-1, occupancy=0):
+        L.check(L.lib().rc_set_launch(self.ctx, rays_per_thread, block_threads, sort_bands, occupancy), self.ctx)
+
+    def get_launch(self):
+        """(rays_per_thread, block_threads, sort_bands, occupancy)"""
+        a, b, c, d = C.c_int(), C.c_int(), C.c_int(), C.c_int()
+        L.check(L.lib().rc_get_launch(self.ctx, C.byref(a), C.byref(b), C.byref(c), C.byref(d)), self.ctx)
+        return a.value, b.value, c.value, d.value
+
+    def solve_async(self, T: np.ndarray, zstart: int = 1) -> int:
+        T = np.ascontiguousarray(T, dtype=np.float32)
+        assert T.shape == field_shape(self.p), (T.shape, field_shape(self.p))
+        t = C.c_int32()
+        L.check(L.lib().rc_solve_async(self.ctx, T.ctypes.data_as(C.POINTER(C.c_float)), zstart, C.byref(t)),
+                self.ctx)
+        return t.value
+
+    def solve_device_async(self, T_dev_ptr: int, zstart: int = 1) -> int:
+        t = C.c_int32()
+        L.check(L.lib().rc_solve_device_async(self.ctx, C.c_void_p(T_dev_ptr), zstart, C.byref(t)), self.ctx)
+        return t.value
+
+    def collect(self, ticket: int, want64: bool = True) -> Result:
+        p = self.p
+        kl = p.kmax // p.p_col
+        Q = np.zeros(result_shape(p), np.float32)
+        S = np.zeros(result_shape(p), np.float32)
+        q64 = np.zeros((kl, p.jmax, p.imax)) if want64 else None
+        v64 = np.zeros((kl, p.jmax, p.imax)) if want64 else None
+        qw = np.zeros((2, kl, p.jmax)) if want64 else None
+        vw = np.zeros((2, kl, p.jmax)) if want64 else None
+        fp = lambda a: a.ctypes.data_as(C.POINTER(C.c_float))
+        dp = lambda a: a.ctypes.data_as(C.POINTER(C.c_double)) if a is not None else None
+        L.check(L.lib().rc_collect(self.ctx, ticket, fp(Q), fp(S), dp(q64), dp(v64), dp(qw), dp(vw)), self.ctx)
+        return Result(Q, S, q64, v64, qw, vw)
+
+    def collect_into(self, ticket: int, Q: np.ndarray, S: np.ndarray):
+        fp = lambda a: a.ctypes.data_as(C.POINTER(C.c_float))
+        L.check(L.lib().rc_collect(self.ctx, ticket, fp(Q), fp(S), None, None, None, None), self.ctx)
+
+    def wait_device(self, ticket: int):
+        q = C.c_void_p()
+        L.check(L.lib().rc_device_results(self.ctx, ticket, C.byref(q), None, None, None), self.ctx)
+        return q.value
+
+    def release(self, ticket: int):
+        L.check(L.lib().rc_collect(self.ctx, ticket, None, None, None, None, None, None), self.ctx)
+
+    def info(self, ticket: int) -> L.RcSolveInfo:
+        i = L.RcSolveInfo()
+        L.check(L.lib().rc_solve_info_get(self.ctx, ticket, C.byref(i)), self.ctx)
+        return i
+
+    def solve(self, T, zstart=1, want64=True) -> Result:
+        return self.collect(self.solve_async(T, zstart), want64)
+
+    def trace(self, ticket, ids, max_cells=0):
+        n = len(ids)
+        arr = (L.RcBundleId * n)(*[L.RcBundleId(*b) for b in ids])
+        out = (L.RcTraceRec * n)()
+        cells = np.full((n, max(max_cells, 1), 4), -1, np.int32)
+        L.check(L.lib().rc_trace(self.ctx, ticket, n, arr, out, max_cells,
+                                 cells.ctypes.data_as(C.POINTER(C.c_int)) if max_cells > 0 else None), self.ctx)
+        return list(out), cells[:, :max_cells]
+
+    def autotune(self, T, zstart=1, pilot_photmax=16):
+        T = np.ascontiguousarray(T, dtype=np.float32)
+        a, b, c = C.c_int(), C.c_int(), C.c_int()
+        L.check(L.lib().rc_autotune(self.ctx, T.ctypes.data_as(C.POINTER(C.c_float)), zstart, pilot_photmax,
+                                    C.byref(a), C.byref(b), C.byref(c)), self.ctx)
+        return a.value, b.value, c.value
+
+    def close(self):
+        if self.ctx:
+            L.lib().rc_destroy(self.ctx)
+            self.ctx = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Batch:
+    """Many solves of uneven size in one persistent launch (rc_batch_*)."""
+
+    def __init__(self, device=0, use_graph=True):
+        self.h = C.c_void_p()
+        L.check(L.lib().rc_batch_create(device, 1 if use_graph else 0, C.byref(self.h)))
+        self.members = []
+
+    def add(self, solver: Solver, T: np.ndarray, zstart: int = 1):
+        T = np.ascontiguousarray(T, dtype=np.float32)
+        self.members.append((solver, T))
+        L.check(L.lib().rc_batch_add(self.h, solver.ctx, T.ctypes.data_as(C.POINTER(C.c_float)), zstart))
+
+    def run(self):
+        L.check(L.lib().rc_batch_run(self.h))
+
+    def wait(self) -> float:
+        ms = C.c_float()
+        L.check(L.lib().rc_batch_wait(self.h, C.byref(ms)))
+        return ms.value
+
+    def collect(self, index, want64=True) -> Result:
+        s, _ = self.members[index]
+        p = s.p
+        kl = p.kmax // p.p_col
+        Q = np.zeros(result_shape(p), np.float32)
+        S = np.zeros(result_shape(p), np.float32)
+        q64 = np.zeros((kl, p.jmax, p.imax)) if want64 else None
+        v64 = np.zeros((kl, p.jmax, p.imax)) if want64 else None
+        qw = np.zeros((2, kl, p.jmax)) if want64 else None
+        vw = np.zeros((2, kl, p.jmax)) if want64 else None
+        fp = lambda a: a.ctypes.data_as(C.POINTER(C.c_float))
+        dp = lambda a: a.ctypes.data_as(C.POINTER(C.c_double)) if a is not None else None
+        L.check(L.lib().rc_batch_collect(self.h, index, fp(Q), fp(S), dp(q64), dp(v64), dp(qw), dp(vw)))
+        return Result(Q, S, q64, v64, qw, vw)
+
+    def close(self):
+        if self.h:
+            L.lib().rc_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -1,0 +1,518 @@
+// rc_kernels.cuh -- kernels of one solve: set-up (Tmax, table rows, grey
+// tables), multigrid temperature levels, the persistent march kernel and
+// the tally.  Included once, by rc_solver.cu.
+#pragma once
+#include "rc_device.cuh"
+
+namespace rc {
+
+// ---------------------------------------------------------------------------
+// set-up
+// ---------------------------------------------------------------------------
+
+// Max of interior T and of the x-wall face averages (mc_gpu_noint.cu:696-710),
+// min of interior T, and finiteness flags.
+__global__ void k_tmax(const float *__restrict__ T, int imax, int jmax, int kmax, DScalars *sc) {
+    const long long n = (long long)imax * jmax * kmax;
+    float mx = 0.f, mn = 3.4e38f;
+    int st = 0;
+    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < n; c += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(c % imax) + 1;
+        const long long r = c / imax;
+        const int j = (int)(r % jmax) + 1;
+        const int k = (int)(r / jmax) + 1;
+        const long long base = (long long)(imax + 2) * (j + (long long)(jmax + 2) * k);
+        const float v = T[base + i];
+        if (!isfinite(v)) {
+            st |= 2;
+            continue;
+        }
+        if (v <= 0.f) st |= 4;
+        mx = fmaxf(mx, v);
+        mn = fminf(mn, v);
+        if (i == 1) {
+            const float f = (T[base] + T[base + 1]) * 0.5f;
+            if (isfinite(f)) mx = fmaxf(mx, f);
+            else st |= 2;
+        }
+        if (i == imax) {
+            const float f = (T[base + imax] + T[base + imax + 1]) * 0.5f;
+            if (isfinite(f)) mx = fmaxf(mx, f);
+            else st |= 2;
+        }
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+        mn = fminf(mn, __shfl_xor_sync(0xffffffffu, mn, o));
+        st |= __shfl_xor_sync(0xffffffffu, st, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        atomicMax(&sc->tmax_bits, __float_as_uint(fmaxf(mx, 0.f)));
+        atomicMin(&sc->tmin_bits, __float_as_uint(fmaxf(mn, 0.f)));
+        if (st) atomicOr(&sc->status, st);
+    }
+}
+
+// Scalars of the solve (mc_gpu_noint.cu:74, 820-826, 1362-1366;
+// read_tables.cpp:36-38, 102-110).  One warp.
+template <typename R>
+__global__ void k_setup1(DScalars *sc, R *Tnb, const R *kP, int nT, int grey, float Tmins, float abscoeff,
+                         double stefan, int photmax, float eps_w, float eps_e) {
+    const float Tmax_f = __uint_as_float(sc->tmax_bits);
+    const R Tmax = (R)Tmax_f;
+    if (grey) {
+        for (int i = threadIdx.x; i < nT; i += blockDim.x)
+            Tnb[i] = (R)((double)Tmins * 0.9 + ((double)Tmax * 1.1 - (double)Tmins * 0.9) * (double)(R)i / (double)(R)nT);
+    }
+    __syncwarp();
+    if (threadIdx.x != 0) return;
+    int status = sc->status;
+    int tm = (int)((Tmax - Tnb[0]) / (Tnb[1] - Tnb[0]));
+    if (tm < 0) {
+        tm = 0;
+        status |= 1;
+    }
+    if (tm > nT - 2) {
+        tm = nT - 2;
+        status |= 1;
+    }
+    const float Tmin_f = __uint_as_float(sc->tmin_bits);
+    if ((R)Tmin_f < Tnb[0] || Tmax > Tnb[nT - 1]) status |= 1;
+    const int row = ((Tmax - Tnb[tm]) < (Tnb[tm + 1] - Tmax)) ? tm : tm + 1;
+    R kappamax;
+    if (grey) kappamax = (R)abscoeff;
+    else kappamax = (kP[tm + 1] - kP[tm]) / (Tnb[tm + 1] - Tnb[tm]) * (Tmax - Tnb[tm]) + kP[tm];
+    const R T4 = Tmax * Tmax * Tmax * Tmax;
+    const R kf = (R)4 * kappamax * T4;
+    sc->tm = tm;
+    sc->row = row;
+    sc->status = status;
+    sc->Tmax = (double)Tmax;
+    sc->kappamax = (double)kappamax;
+    sc->Ibmax_f = (double)(R)((double)kf * stefan / (double)photmax);
+    sc->Ibmax_w[0] = (double)(R)((double)eps_w * stefan * (double)T4 / (double)photmax);
+    sc->Ibmax_w[1] = (double)(R)((double)eps_e * stefan * (double)T4 / (double)photmax);
+    const R T0 = Tnb[0];
+    const R inv_dT = (R)1 / (Tnb[1] - Tnb[0]);
+    sc->T0 = (double)T0;
+    sc->inv_dT = (double)inv_dT;
+    sc->Pm = (double)table_coord(Tmax, T0, inv_dT, nT);
+}
+
+__global__ void k_init_scalars(DScalars *sc) {
+    if (threadIdx.x == 0 && blockIdx.x == 0) {
+        DScalars z;
+        memset(&z, 0, sizeof(z));
+        z.tmax_bits = 0u;
+        z.tmin_bits = 0x7f800000u;
+        *sc = z;
+    }
+}
+
+// Grey-gas Planck table I_b(Tnb[t], wvc[b]) (read_tables.cpp:140-148).
+template <typename R>
+__global__ void k_grey_ib(R *Ibt, const R *Tnb, const R *wvc, int nT, int nB) {
+    const int n = nT * nB;
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += gridDim.x * blockDim.x) {
+        const int b = e / nT, t = e % nT;
+        Ibt[e] = (R)rc_planck((double)Tnb[t], (double)wvc[b]);
+    }
+}
+
+// Cumulative Planck band probability of one table row
+// (read_tables.cpp:153-165 grey, :204-218 walls).
+template <typename R>
+__device__ void planck_cdf_row(R *out, const R *Ibt, const R *wvl, const R *wvr, int nT, int nB, int row) {
+    R c = Ibt[(size_t)0 * nT + row] * (wvr[0] - wvl[0]) * (R)100;
+    out[0] = c;
+    for (int b = 1; b < nB; ++b) {
+        c = c + Ibt[(size_t)b * nT + row] * (wvr[b] - wvl[b]) * (R)100;
+        out[b] = c;
+    }
+    const R last = out[nB - 1];
+    for (int b = 0; b < nB; ++b) out[b] = out[b] / last;
+}
+
+// Band CDF rows at the row nearest Tmax: fluid (copy, or the grey Planck
+// CDF) and walls (readS).
+template <typename R>
+__global__ void k_setup2(const DScalars *sc, R *cdf_f, R *cdf_s, const R *prob, const R *Ibt, const R *wvl,
+                         const R *wvr, int nT, int nB, int grey, int walls) {
+    const int row = sc->row;
+    if (!grey) {
+        for (int b = threadIdx.x; b < nB; b += blockDim.x) cdf_f[b] = prob[(size_t)row * nB + b];
+    }
+    if (threadIdx.x == 0 && grey) planck_cdf_row(cdf_f, Ibt, wvl, wvr, nT, nB, row);
+    if (threadIdx.x == 32 % blockDim.x && walls) planck_cdf_row(cdf_s, Ibt, wvl, wvr, nT, nB, row);
+}
+
+// Texture-space trilinear sample of the float field with clamped indices
+// (the reference's tex3D with cudaFilterModeLinear/cudaAddressModeClamp,
+// memory_copy_noint.cu:159-165), with exact float weights.
+__device__ __forceinline__ float tex_sample(const float *T, int nx, int ny, int nz, float x, float y, float z) {
+    const float xb = x - 0.5f, yb = y - 0.5f, zb = z - 0.5f;
+    const float fx = floorf(xb), fy = floorf(yb), fz = floorf(zb);
+    const float ax = xb - fx, ay = yb - fy, az = zb - fz;
+    int i0 = (int)fx, j0 = (int)fy, k0 = (int)fz;
+    int i1 = i0 + 1, j1 = j0 + 1, k1 = k0 + 1;
+    i0 = min(max(i0, 0), nx - 1);
+    i1 = min(max(i1, 0), nx - 1);
+    j0 = min(max(j0, 0), ny - 1);
+    j1 = min(max(j1, 0), ny - 1);
+    k0 = min(max(k0, 0), nz - 1);
+    k1 = min(max(k1, 0), nz - 1);
+    auto at = [&](int i, int j, int k) { return T[(size_t)i + (size_t)nx * ((size_t)j + (size_t)ny * k)]; };
+    const float c00 = at(i0, j0, k0) * (1.f - ax) + at(i1, j0, k0) * ax;
+    const float c10 = at(i0, j1, k0) * (1.f - ax) + at(i1, j1, k0) * ax;
+    const float c01 = at(i0, j0, k1) * (1.f - ax) + at(i1, j0, k1) * ax;
+    const float c11 = at(i0, j1, k1) * (1.f - ax) + at(i1, j1, k1) * ax;
+    const float c0 = c00 * (1.f - ay) + c10 * ay;
+    const float c1 = c01 * (1.f - ay) + c11 * ay;
+    return c0 * (1.f - az) + c1 * az;
+}
+
+// One array of the multigrid temperature pyramid: the cell temperatures
+// of a level (sampled at the coarse cell centre, mc_gpu_noint.cu:334-338)
+// or the emission temperature of a wall at that level (:392-396, 468-472).
+struct LevelJob {
+    void *dst;
+    int type;     // 0 cells, 1 + w: wall w
+    int im, jm, km;
+    int rx, ry, rz;   // fine cells per level cell (imax/im ...)
+    int face;     // wall sampled at the face (1) or at the first cell (0)
+    long long n, start;
+};
+constexpr int kMaxJobs = RC_MAX_LEVELS * 7 + 2;
+struct LevelJobs {
+    LevelJob job[kMaxJobs];
+    int njobs;
+    long long total;
+};
+
+template <typename R>
+__global__ void k_levels(const float *__restrict__ T, int imax, int jmax, int kmax, LevelJobs jobs,
+                         const DScalars *sc, int nT) {
+    const int nx = imax + 2, ny = jmax + 2, nz = kmax + 2;
+    const R T0 = (R)sc->T0, inv_dT = (R)sc->inv_dT;
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < jobs.total;
+         e += (long long)gridDim.x * blockDim.x) {
+        int jb = 0;
+        while (jb + 1 < jobs.njobs && jobs.job[jb + 1].start <= e) ++jb;
+        const LevelJob &J = jobs.job[jb];
+        const long long l = e - J.start;
+        R *dst = (R *)J.dst;
+        const float rxf = (float)J.rx, ryf = (float)J.ry, rzf = (float)J.rz;
+        if (J.type == 0) {
+            const int ic = (int)(l % J.im) + 1;
+            const long long r = l / J.im;
+            const int jc = (int)(r % J.jm) + 1;
+            const int kc = (int)(r / J.jm) + 1;
+            const float t1 = ((float)ic - 0.5f) * rxf + 1.0f;
+            const float t2 = ((float)jc - 0.5f) * ryf + 1.0f;
+            const float t3 = ((float)kc - 0.5f) * rzf + 1.0f;
+            dst[l] = table_coord((R)tex_sample(T, nx, ny, nz, t1, t2, t3), T0, inv_dT, nT);
+        } else {
+            const int w = J.type - 1;
+            float x, y, z;
+            if (w <= RC_EAST) {
+                const int jc = (int)(l % J.jm) + 1, kc = (int)(l / J.jm) + 1;
+                y = ((float)jc - 0.5f) * ryf + 1.0f;
+                z = ((float)kc - 0.5f) * rzf + 1.0f;
+                x = (w == RC_WEST) ? (J.face ? 1.0f : 1.5f) : (J.face ? (float)imax + 1.0f : (float)imax + 0.5f);
+            } else if (w <= RC_NORTH) {
+                const int ic = (int)(l % J.im) + 1, kc = (int)(l / J.im) + 1;
+                x = ((float)ic - 0.5f) * rxf + 1.0f;
+                z = ((float)kc - 0.5f) * rzf + 1.0f;
+                y = (w == RC_SOUTH) ? (J.face ? 1.0f : 1.5f) : (J.face ? (float)jmax + 1.0f : (float)jmax + 0.5f);
+            } else {
+                const int ic = (int)(l % J.im) + 1, jc = (int)(l / J.im) + 1;
+                x = ((float)ic - 0.5f) * rxf + 1.0f;
+                y = ((float)jc - 0.5f) * ryf + 1.0f;
+                z = (w == RC_BOT) ? (J.face ? 1.0f : 1.5f) : (J.face ? (float)kmax + 1.0f : (float)kmax + 0.5f);
+            }
+            dst[l] = table_coord((R)tex_sample(T, nx, ny, nz, x, y, z), T0, inv_dT, nT);
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// march: persistent warps over tiles of 32 work items
+// ---------------------------------------------------------------------------
+//
+// A work item is one chunk of rays_per_thread consecutive bundles of one
+// (cell, replicate).  A warp takes a tile of 32 items, i.e. a pool of
+// 32*rays_per_thread bundles:
+//   * the 32 items are decoded once, one per lane;
+//   * bundles are emitted in converged waves of 32 (all lanes run the
+//     Philox draws, direction, band/g bisection and OERM weights together)
+//     into a per-warp ring in shared memory, whenever the ring holds fewer
+//     than 32 bundles;
+//   * every lane traces one ray; when its ray ends it takes the next
+//     emitted bundle from the ring (warp ballot + prefix count), so lanes
+//     never wait for each other while the pool has bundles;
+//   * each bundle's FP64 tally goes to its own shared-memory slot; at the end
+//     of the tile the slots are summed in bundle order, so the result does
+//     not depend on which lane traced which bundle.
+
+struct MarchArgs {
+    const void *solves;          // DSolve<R>[nsolves]
+    const long long *tile_start; // [nsolves+1] exclusive prefix of tiles
+    int nsolves;
+    long long total_tiles;
+    unsigned long long *tile_counter;
+    int rpt_max;
+};
+
+template <typename R>
+struct WarpShared {
+    DSolve<R> sd;
+    ItemId items[kWarp];
+    Emitted<R> ring[kRing];
+};
+
+template <typename R>
+__device__ __forceinline__ void load_solve(DSolve<R> *dst, const DSolve<R> *src, int lane) {
+    const int *s = reinterpret_cast<const int *>(src);
+    int *d = reinterpret_cast<int *>(dst);
+    constexpr int nw = (int)(sizeof(DSolve<R>) / 4);
+    for (int w = lane; w < nw; w += kWarp) d[w] = s[w];
+    __syncwarp();
+    if (lane == 0) {
+        const DScalars *sc = dst->sc;
+        dst->Pm = (R)sc->Pm;
+        dst->Ibmax_f = (R)sc->Ibmax_f;
+        dst->Ibmax_w0 = (R)sc->Ibmax_w[0];
+        dst->Ibmax_w1 = (R)sc->Ibmax_w[1];
+        dst->row = sc->row;
+    }
+    __syncwarp();
+}
+
+// MINB: resident 256-thread blocks per SM the register allocation must
+// allow (2: up to 128 registers, 3: 80, 4: 64).
+template <typename R, int MINB>
+__global__ void __launch_bounds__(256, MINB) k_march(MarchArgs a) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+    WarpShared<R> *ws = reinterpret_cast<WarpShared<R> *>(smem) + warp;
+    const size_t wbytes = ((sizeof(WarpShared<R>) * nwarps) + 15) & ~(size_t)15;
+    double *slots = reinterpret_cast<double *>(smem + wbytes) + (size_t)warp * kWarp * a.rpt_max;
+    const DSolve<R> *solves = reinterpret_cast<const DSolve<R> *>(a.solves);
+    const unsigned lt = (1u << lane) - 1u;
+    int cur = -1;
+    for (;;) {
+        unsigned long long tile = 0;
+        if (lane == 0) tile = atomicAdd(a.tile_counter, 1ull);
+        tile = __shfl_sync(0xffffffffu, tile, 0);
+        if (tile >= (unsigned long long)a.total_tiles) break;
+        int lo = 0, hi = a.nsolves;
+        while (hi - lo > 1) {
+            const int mid = (lo + hi) >> 1;
+            if ((unsigned long long)a.tile_start[mid] <= tile) lo = mid;
+            else hi = mid;
+        }
+        if (lo != cur) {
+            load_solve(&ws->sd, solves + lo, lane);
+            cur = lo;
+        }
+        const DSolve<R> &S = ws->sd;
+        const long long item0 = (long long)(tile - (unsigned long long)a.tile_start[lo]) * kWarp;
+        const int rpt = S.rpt;
+        const int lrpt = __ffs(rpt) - 1;  // rpt is a power of two
+        const int pool = kWarp * rpt;
+        ws->items[lane] = decode_item(S, item0 + lane);
+        for (int b = lane; b < pool; b += kWarp) slots[b] = 0.0;
+        __syncwarp();
+        int next_b = 0, head = 0, count = 0;
+        bool active = false;
+        int myb = 0;
+        unsigned int nsteps = 0, nbund = 0;
+        Ray<R> r;
+        for (;;) {
+            if (count < kWarp && next_b < pool) {
+                // converged emission wave: one bundle per lane
+                const int b = next_b + lane;
+                Emitted<R> e;
+                bool ok = false;
+                if (b < pool) {
+                    const ItemId it = ws->items[b >> lrpt];
+                    const int h = it.h0 + (b & (rpt - 1));
+                    if (it.kind >= 0 && h < S.photmax) {
+                        nbund++;
+                        ok = emit_bundle(e, S, it.kind, it.i, it.j, it.k, it.v, h);
+                        e.b = b;
+                    }
+                }
+                const unsigned m = __ballot_sync(0xffffffffu, ok);
+                if (ok) ws->ring[(head + count + __popc(m & lt)) & (kRing - 1)] = e;
+                count += __popc(m);
+                next_b += kWarp;
+                __syncwarp();
+            }
+            const bool need = !active;
+            const unsigned m = __ballot_sync(0xffffffffu, need);
+            const int navail = min(count, __popc(m));
+            if (need) {
+                const int rank = __popc(m & lt);
+                if (rank < navail) {
+                    const Emitted<R> e = ws->ring[(head + rank) & (kRing - 1)];
+                    const ItemId it = ws->items[e.b >> lrpt];
+                    place_bundle(r, S, e, it.kind, it.i, it.j, it.k);
+                    myb = e.b;
+                    active = level_advance(r, S);
+                    if (!active) slots[myb] = r.De;
+                }
+            }
+            head = (head + navail) & (kRing - 1);
+            count -= navail;
+            if (!__any_sync(0xffffffffu, active) && count == 0 && next_b >= pool) break;
+            if (active) {
+                march_step(r, S, S.lev[r.lev]);
+                nsteps++;
+                bool done = !(r.tra > r.tol);
+                if (!done) done = !level_advance(r, S);
+                if (done) {
+                    slots[myb] = r.De;
+                    active = false;
+                }
+            }
+            __syncwarp();
+        }
+        __syncwarp();
+        // chunk sum of this lane's item, then group sums in item order
+        double s = 0.0;
+        for (int h = 0; h < rpt; ++h) s += slots[lane * rpt + h];
+        const int gs = S.gsize;
+        const int base = (lane / gs) * gs;
+        double g = 0.0;
+        for (int q = 0; q < gs; ++q) g += __shfl_sync(0xffffffffu, s, base + q);
+        const long long item = item0 + lane;
+        if (lane == base && item < S.n_items) S.partial[item / gs] = g;
+        // counters
+        unsigned long long st = nsteps, nb = nbund;
+        for (int o = 16; o > 0; o >>= 1) {
+            st += __shfl_xor_sync(0xffffffffu, st, o);
+            nb += __shfl_xor_sync(0xffffffffu, nb, o);
+        }
+        if (lane == 0) {
+            atomicAdd(&S.sc->steps, st);
+            atomicAdd(&S.sc->bundles, nb);
+        }
+        __syncwarp();
+    }
+}
+
+template <typename R>
+constexpr size_t march_smem_bytes(int block, int rpt_max) {
+    return ((((size_t)sizeof(WarpShared<R>) * (block / kWarp)) + 15) & ~(size_t)15) +
+           (size_t)(block / kWarp) * kWarp * rpt_max * sizeof(double);
+}
+
+// ---------------------------------------------------------------------------
+// tally: replicate sums -> mean and variance (kernel_fluid :229-239,
+// kernel_surface :1468-1478), compact outputs
+// ---------------------------------------------------------------------------
+template <typename R>
+__global__ void k_tally(const DSolve<R> *Sp, double *q64, double *var64, double *qw64, double *vw64, float *Qc,
+                        float *Sc, float *Wq, float *Ws) {
+    const DSolve<R> &S = *Sp;
+    const long long ncf = (long long)S.imax * S.jmax * S.kloc;
+    const long long ncw = (long long)S.nwalls * S.jmax * S.kloc;
+    const int nVar = S.nVar, np = S.nparts;
+    double a = 0.0;
+    if (nVar > 1) {
+        a = 1. / (nVar - 0.5);
+        a = a * 1. / (nVar - 1);
+    }
+    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < ncf + ncw;
+         c += (long long)gridDim.x * blockDim.x) {
+        const double *p = S.partial + c * nVar * np;
+        double sum = 0.0;
+        for (int v = 0; v < nVar; ++v) {
+            double dv = 0.0;
+            for (int q = 0; q < np; ++q) dv += p[v * np + q];
+            sum += dv;
+        }
+        const double mean = sum / nVar;
+        double var = 0.0;
+        for (int v = 0; v < nVar; ++v) {
+            double dv = 0.0;
+            for (int q = 0; q < np; ++q) dv += p[v * np + q];
+            const double d = dv - mean;
+            var += a * d * d;
+        }
+        if (c < ncf) {
+            if (q64) q64[c] = mean;
+            if (var64) var64[c] = var;
+            Qc[c] = (float)mean;
+            Sc[c] = (float)sqrt(var);
+        } else {
+            const long long cw = c - ncf;
+            const long long nwc = (long long)S.jmax * S.kloc;
+            const int slot = (int)(cw / nwc);
+            const long long o = (long long)S.wall_id[slot] * nwc + (cw % nwc);
+            if (qw64) qw64[o] = mean;
+            if (vw64) vw64[o] = var;
+            Wq[o] = (float)mean;
+            Ws[o] = (float)sqrt(var);
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// bundle traces: one thread per requested bundle, same device functions
+// ---------------------------------------------------------------------------
+template <typename R>
+__global__ void k_trace(const DSolve<R> *Sp, int n, const rc_bundle_id *ids, rc_trace_rec *out, int max_cells,
+                        int *cells) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    DSolve<R> S = *Sp;
+    const DScalars *sc = S.sc;
+    S.Pm = (R)sc->Pm;
+    S.Ibmax_f = (R)sc->Ibmax_f;
+    S.Ibmax_w0 = (R)sc->Ibmax_w[0];
+    S.Ibmax_w1 = (R)sc->Ibmax_w[1];
+    S.row = sc->row;
+    const rc_bundle_id id = ids[t];
+    rc_trace_rec rec;
+    rec.nb = rec.g = -1;
+    rec.nsteps = 0;
+    rec.end_level = 0;
+    rec.sx = rec.sy = rec.sz = 0.f;
+    rec.tra = 0.f;
+    rec.De = 0.0;
+    Emitted<R> e;
+    const bool ok = emit_bundle(e, S, id.kind, id.i, id.j, id.k, id.v, id.h);
+    rec.nb = e.nbg & 0xfffff;
+    rec.g = e.nbg >> 20;
+    rec.sx = (float)e.sx;
+    rec.sy = (float)e.sy;
+    rec.sz = (float)e.sz;
+    if (ok) {
+        Ray<R> r;
+        place_bundle(r, S, e, id.kind, id.i, id.j, id.k);
+        bool active = level_advance(r, S);
+        int ns = 0;
+        while (active) {
+            if (ns < max_cells && cells) {
+                int *c = cells + ((size_t)t * max_cells + ns) * 4;
+                c[0] = r.lev;
+                c[1] = r.ic;
+                c[2] = r.jc;
+                c[3] = r.kc;
+            }
+            march_step(r, S, S.lev[r.lev]);
+            ns++;
+            active = r.tra > r.tol;
+            if (active) active = level_advance(r, S);
+        }
+        rec.nsteps = ns;
+        rec.end_level = r.lev;
+        rec.tra = (float)r.tra;
+        rec.De = r.De;
+    }
+    out[t] = rec;
+}
+
+}  // namespace rc
