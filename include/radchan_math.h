@@ -153,10 +153,17 @@ RC_HD float rc_expf(float x) {
     return p * rc_exp2i_f((int)n);
 }
 
-/* e^x - 1 without cancellation near 0. */
+/* e^x - 1 without cancellation near 0, branch-free:
+ * e^x - 1 = 2^n (e^r - 1) + (2^n - 1), evaluated as one fused multiply-add.
+ * For |x| < ln2/2, n = 0 and the result is the polynomial itself.
+ * Arguments are clamped to [-87, 88] (e^-87 - 1 rounds to -1). */
 RC_HD float rc_expm1f(float x) {
-    if (x > -0.34657359f && x < 0.34657359f) return rc_expm1_poly_f(x);
-    return rc_expf(x) - 1.0f;
+    x = fminf(fmaxf(x, -87.0f), 88.0f);
+    float n = rintf(x * RC_LOG2E_F);
+    float r = (x - n * RC_LN2_HI_F) - n * RC_LN2_LO_F;
+    float p = rc_expm1_poly_f(r);
+    float s = rc_exp2i_f((int)n);
+    return fmaf(s, p, s - 1.0f);
 }
 
 /* ------------------------------------------------------------------ */
@@ -201,8 +208,12 @@ RC_HD double rc_exp(double x) {
 }
 
 RC_HD double rc_expm1(double x) {
-    if (x > -0.34657359027997264 && x < 0.34657359027997264) return rc_expm1_poly_d(x);
-    return rc_exp(x) - 1.0;
+    x = fmin(fmax(x, -708.0), 709.0);
+    double n = rint(x * RC_LOG2E_D);
+    double r = (x - n * RC_LN2_HI_D) - n * RC_LN2_LO_D;
+    double p = rc_expm1_poly_d(r);
+    double s = rc_exp2i_d((int)n);
+    return fma(s, p, s - 1.0);
 }
 
 /* ------------------------------------------------------------------ */

@@ -106,13 +106,19 @@ float tex3(const std::vector<float> &T, int nx, int ny, int nz, float x, float y
     return c0 * (1.f - az) + c1 * az;
 }
 
+// Table coordinate with 8 fractional bits (the weight precision of the
+// reference's texture filtering): q = rint(256 clamp((T - T0)/dT, 0, nT-1)).
 template <typename R>
-R lerpT(const R *col, int nT, R pos) {
-    R p = std::min(std::max(pos, (R)0), (R)(nT - 1));
-    if (p != p) p = (R)0;
-    int i0 = (int)p;
+int tcoord(R T, R T0, R inv_dT, int nT) {
+    R p = std::fmin(std::fmax((T - T0) * inv_dT, (R)0), (R)(nT - 1));
+    return (int)std::rint(p * (R)256);
+}
+
+template <typename R>
+R lerpq(const R *col, int nT, int q) {
+    int i0 = q >> 8;
     int i1 = std::min(i0 + 1, nT - 1);
-    R a = p - (R)i0;
+    R a = (R)(q & 255) * (R)0.00390625;
     return col[i0] * ((R)1 - a) + col[i1] * a;
 }
 
@@ -409,7 +415,7 @@ struct Problem {
                 else if (w <= RC_NORTH) idx = (ray.kc - 1) * G.im + (ray.ic - 1);
                 else idx = (ray.jc - 1) * G.im + (ray.ic - 1);
                 R Tw = Twl[lev][w][idx];
-                deposit(ray, De, Ibmax, ratioI, invTi4, lerpT(ibcol, nT, (Tw - T0) * inv_dT));
+                deposit(ray, De, Ibmax, ratioI, invTi4, lerpq(ibcol, nT, tcoord(Tw, T0, inv_dT, nT)));
                 break;
             }
             case 3: {  // specular reflection, on the component normal to the wall
@@ -460,9 +466,9 @@ struct Problem {
             R dsy = (fyu - ray.yp) * ray.isy;
             R dsz = (fzu - ray.zp) * ray.isz;
             R tf = Tcell(lev, ray.ic, ray.jc, ray.kc);
-            R pos = (tf - T0) * inv_dT;
-            R absco = lerpT(kcol, nT, pos);
-            R blackpow = lerpT(ibcol, nT, pos);
+            int q = tcoord(tf, T0, inv_dT, nT);
+            R absco = lerpq(kcol, nT, q);
+            R blackpow = lerpq(ibcol, nT, q);
             R ds = dsx;
             if (ds > dsy) ds = dsy;
             if (ds > dsz) ds = dsz;
@@ -600,17 +606,22 @@ struct Problem {
         }
         const R *kcol = &kt[((size_t)nb * nQ + g) * nT];
         const R *ibcol = &Ibt[(size_t)nb * nT];
-        R pos_i = (Ti - T0) * inv_dT, pos_m = (Tmax - T0) * inv_dT;
-        R Ib_i = lerpT(ibcol, nT, pos_i), Ib_m = lerpT(ibcol, nT, pos_m);
-        if (!(Ib_i > 0) || !(Ib_m > 0)) return 0.0;
+        // OERM weights: ratioI = Ib(Ti) k(Ti) / (Ib(Tmax) k(Tmax)) for the fluid
+        // (mc_gpu_noint.cu:180-186), Ib(Ti)/Ib(Tmax) for walls (:1421-1424)
+        int pos_i = tcoord(Ti, T0, inv_dT, nT), pos_m = tcoord(Tmax, T0, inv_dT, nT);
+        R Ib_i = lerpq(ibcol, nT, pos_i);
+        if (!(Ib_i > 0)) return 0.0;
         R invTi4 = (R)1 / Ib_i;
         R ratioI;
         if (kind == 0) {
-            R k_i = lerpT(kcol, nT, pos_i), k_m = lerpT(kcol, nT, pos_m);
-            if (!(k_m > 0)) return 0.0;
-            ratioI = ((((R)1 / invTi4) / Ib_m) * k_i) / k_m;
+            R k_i = lerpq(kcol, nT, pos_i);
+            R den = lerpq(ibcol, nT, pos_m) * lerpq(kcol, nT, pos_m);
+            if (!(den > 0)) return 0.0;
+            ratioI = (Ib_i * k_i) / den;
         } else {
-            ratioI = ((R)1 / invTi4) / Ib_m;
+            R Ib_m = lerpq(ibcol, nT, pos_m);
+            if (!(Ib_m > 0)) return 0.0;
+            ratioI = Ib_i / Ib_m;
             const Grid &G = grid[0];
             if (ray.flag[0] && ray.xp == (R)G.xu[ray.ic - 1]) ray.ic = ray.ic - 1;
             if (ray.flag[1] && ray.yp == (R)G.yu[ray.jc - 1]) ray.jc = ray.jc - 1;

@@ -34,7 +34,9 @@
 namespace rc {
 
 constexpr int kWarp = 32;
-constexpr int kRing = 64;  // per-warp ring of emitted bundles (two waves)
+constexpr int kRing = 64;    // per-warp ring of emitted bundles (two waves)
+constexpr int kGuide = 256;  // buckets of the band-CDF guide tables
+constexpr int kFeedIdle = 8; // idle lanes that make a warp leave its step loop to take new bundles
 
 // ---------------------------------------------------------------------------
 // descriptors
@@ -42,10 +44,18 @@ constexpr int kRing = 64;  // per-warp ring of emitted bundles (two waves)
 template <typename R>
 struct DLevel {
     int im, jm, km, maxs;
-    int rx, ry, rz, pad;      // ratio to the next (coarser) level
+    int rx, ry, rz;           // ratio to the next (coarser) level
+    int nbi, nbj;             // 4x4x4 bricks per x and y row of the coordinate array
     const R *xu, *yu, *zu;    // faces
-    const R *P;               // [km][jm][im] table coordinate of the cell temperature
-    const R *Pw[6];           // wall emission temperature coordinates (or null)
+    const uint16_t *P;        // table coordinate of every cell, 4x4x4 bricks (see cell_index)
+    const uint16_t *Pw[6];    // wall emission temperature coordinates (or null)
+};
+
+// Interleaved table row: k and I_b at temperature rows t and t+1 (the last
+// row repeats itself), so one 16-byte load serves a step's interpolation.
+template <typename R>
+struct alignas(4 * sizeof(R)) KIRow {
+    R k0, ib0, k1, ib1;
 };
 
 // Per-solve scalars written on the device by the set-up kernels.
@@ -57,7 +67,8 @@ struct DScalars {
     int pad;
     double Tmax, kappamax, Ibmax_f, Ibmax_w[2];
     double T0, inv_dT;        // first table temperature and 1/spacing
-    double Pm;                // table coordinate of Tmax
+    int Pm;                   // table coordinate of Tmax
+    int pad2;
     unsigned long long steps, bundles;
 };
 
@@ -74,8 +85,8 @@ struct DSolve {
     R Lx, Ly, Lz;
     R toll, tollS;
     // run-time values (copied from DScalars by the kernels)
-    R Pm, Ibmax_f, Ibmax_w0, Ibmax_w1;
-    int row, pad2;
+    R Ibmax_f, Ibmax_w0, Ibmax_w1;
+    int Pm, row;
     const R *xc, *yc, *zc;    // level-0 cell centres incl. ghosts
     const R *kt;              // [nB][nQ][nT]
     const R *Ibt;             // [nB][nT]
@@ -84,10 +95,18 @@ struct DSolve {
     const R *cdf_s;           // [nB] wall band CDF at the selected row
     const R *probq;           // [nQ]
     const R *Ibw;             // [6][nB] fixed wall spectra
-    const R *Pw0[2];          // level-0 west/east face coordinates [kmax][jmax]
+    const uint16_t *Pw0[2];   // level-0 west/east face coordinates [kmax][jmax]
+    const KIRow<R> *ki;       // [nB][nQ][nT] interleaved k / I_b rows
+    const R *den_f;           // [nB][nQ] I_b(Tmax) k(Tmax) (fluid OERM weight denominator)
+    const R *ibm;             // [nB] I_b(Tmax) (wall OERM weight denominator)
+    const int *guide_f;       // [kGuide] first band with cdf_f > q/kGuide
+    const int *guide_s;       // [kGuide] same for cdf_s
     DScalars *sc;
     double *partial;
     long long n_fluid_items, n_items, n_tiles;
+    // multiply-high reciprocals of the item decomposition divisors
+    unsigned long long mg_nchunk, mg_nvar, mg_imax, mg_jmax, mg_nwc;
+    unsigned long long nwc;   // jmax * kloc
     uint32_t key0, key1;
 };
 
@@ -112,27 +131,60 @@ template <> struct RT<double> {
     static __device__ __forceinline__ double fabs_(double a) { return fabs(a); }
 };
 
-// Table coordinate of a temperature: clamp((T - T0)/dT, 0, nT-1); NaN -> 0.
+// Table coordinate of a temperature with 8 fractional bits, the weight
+// precision of the texture unit the reference interpolates with:
+// q = rint(256 * clamp((T - T0)/dT, 0, nT-1)); NaN -> 0.  nT <= 256.
 template <typename R>
-__device__ __forceinline__ R table_coord(R T, R T0, R inv_dT, int nT) {
-    return RT<R>::fmin_(RT<R>::fmax_((T - T0) * inv_dT, (R)0), (R)(nT - 1));
+__device__ __forceinline__ int table_coord(R T, R T0, R inv_dT, int nT) {
+    const R p = RT<R>::fmin_(RT<R>::fmax_((T - T0) * inv_dT, (R)0), (R)(nT - 1));
+    return (int)rint(p * (R)256);
+}
+
+// One interleaved table row through the read-only path.
+__device__ __forceinline__ KIRow<float> load_row(const KIRow<float> *p) {
+    const float4 v = __ldg(reinterpret_cast<const float4 *>(p));
+    KIRow<float> r;
+    r.k0 = v.x;
+    r.ib0 = v.y;
+    r.k1 = v.z;
+    r.ib1 = v.w;
+    return r;
+}
+__device__ __forceinline__ KIRow<double> load_row(const KIRow<double> *p) {
+    const double2 a = __ldg(reinterpret_cast<const double2 *>(p));
+    const double2 b = __ldg(reinterpret_cast<const double2 *>(p) + 1);
+    KIRow<double> r;
+    r.k0 = a.x;
+    r.ib0 = a.y;
+    r.k1 = b.x;
+    r.ib1 = b.y;
+    return r;
+}
+
+// Fraction of a table coordinate: (q mod 256) / 256, exact.
+template <typename R>
+__device__ __forceinline__ R coord_frac(int q) {
+    return (R)(q & 255) * (R)0.00390625;
+}
+
+// Offset of cell (i,j,k) (1-based) in a 4x4x4-brick array.
+__device__ __forceinline__ int cell_index(int i, int j, int k, int nbi, int nbj) {
+    const int a = i - 1, b = j - 1, c = k - 1;
+    return (((c >> 2) * nbj + (b >> 2)) * nbi + (a >> 2)) * 64 + ((a & 3) | ((b & 3) << 2) | ((c & 3) << 4));
 }
 
 // Linear interpolation in temperature along one table column at a clamped
 // coordinate (the reference does this with a clamped linear-filter texture,
 // mc_gpu_noint.cu:341-345, memory_copy_noint.cu:241-245).
-struct Lerp {
-    int i0, i1;
-};
 template <typename R>
 __device__ __forceinline__ R lerp_at(const R *col, int i0, int i1, R a) {
     return col[i0] * ((R)1 - a) + col[i1] * a;
 }
 template <typename R>
-__device__ __forceinline__ R tab_lerp(const R *col, int nT, R p) {
-    const int i0 = (int)p;
+__device__ __forceinline__ R tab_lerp(const R *col, int nT, int q) {
+    const int i0 = q >> 8;
     const int i1 = min(i0 + 1, nT - 1);
-    return lerp_at(col, i0, i1, p - (R)i0);
+    return lerp_at(col, i0, i1, coord_frac<R>(q));
 }
 
 // Inverse-CDF bisection with the reference's edge rules
@@ -151,10 +203,26 @@ __device__ __forceinline__ int bisect(const R *cdf, int n, R u) {
     return min(r, n - 1);
 }
 
-// A bundle after emission: direction, sampled band/g and OERM weights.
+// Band index of a uniform u on a cumulative table: the first b with
+// u < cdf[b], with the reference's edge rules (R < cdf[0] -> 0, R == 1 ->
+// n-1, mc_gpu_noint.cu:1113-1127).  For a non-decreasing cdf this is the
+// same index the reference's bisection returns; the guide table gives the
+// first band with cdf > q/kGuide, from which a short linear scan finishes.
+template <typename R>
+__device__ __forceinline__ int guided_index(const R *cdf, const int *guide, int n, R u) {
+    const int q = min((int)(u * (R)kGuide), kGuide - 1);
+    int b = guide[q];
+    while (b < n - 1 && !(u < cdf[b])) ++b;
+    return u == (R)1 ? n - 1 : b;
+}
+
+// A bundle after emission, placed at its start point: position, cell,
+// direction, sampled band/g and OERM weights.
 template <typename R>
 struct Emitted {
-    R sx, sy, sz, isx, isy, isz, ratioI, invTi4;
+    R xp, yp, zp, sx, sy, sz, ratioI, invTi4;
+    int ij;    // ic | jc << 16
+    int kk;    // kc | kind << 16
     int nbg;   // nb | g << 20
     int b;     // index in the warp's bundle pool
 };
@@ -166,7 +234,7 @@ struct Ray {
     R isx, isy, isz;
     R tra;
     R Ibmax, ratioI, invTi4, tol;
-    const R *kcol, *ibcol;
+    const KIRow<R> *kicol;
     int ic, jc, kc;
     int fx, fy, fz;
     int lev, counter;
@@ -184,9 +252,14 @@ __device__ __forceinline__ rc_u32x4 bundle_draws(uint32_t key0, uint32_t key1, i
     return rc_philox4x32_10(c, key0, key1);
 }
 
-// Emission of one bundle.  kind 0: fluid cell (i,j,k) (kernel_fluid
-// :115-186); kind 1/2: west/east wall cell (j,k) (kernel_surface
-// :1381-1424).  Returns false if the bundle carries no energy.
+// Emission of one bundle, placed at its start point.  kind 0: fluid cell
+// (i,j,k) from its centre (kernel_fluid :115-186); kind 1/2: west/east wall
+// cell (j,k) from the wall (kernel_surface :1381-1441).  Returns false if
+// the bundle carries no energy.
+//
+// OERM weights: invTi4 = 1/I_b(Ti); ratioI = (I_b(Ti) k(Ti)) / (I_b(Tmax)
+// k(Tmax)) for the fluid (the reference's ((1/invTi4)/Ib(Tmax))*k(Ti)/
+// k(Tmax), :180-186) and I_b(Ti)/I_b(Tmax) for walls (:1421-1424).
 template <typename R>
 __device__ __forceinline__ bool emit_bundle(Emitted<R> &e, const DSolve<R> &S, int kind, int i, int j, int k, int v,
                                             int h) {
@@ -197,27 +270,25 @@ __device__ __forceinline__ bool emit_bundle(Emitted<R> &e, const DSolve<R> &S, i
     const R u_phi = (R)rc_u01(d.x), u_mu = (R)rc_u01(d.y), u_b = (R)rc_u01(d.z), u_g = (R)rc_u01(d.w);
     R sp, cp;
     RT<R>::sincos2pi_(u_phi, &sp, &cp);
-    R Pi;
-    int nb, g;
+    int Pi;
+    int nb, g, ic = i;
+    R st;
+    e.yp = S.yc[j];
+    e.zp = S.zc[k];
     if (kind == 0) {
         // isotropic: cos(theta) = 1 - 2u (emiss_ang, :1077-1084)
         const R mu = (R)1 - (R)2 * u_mu;
-        const R st = RT<R>::sqrt_(((R)1 - mu) * ((R)1 + mu));
+        st = RT<R>::sqrt_(((R)1 - mu) * ((R)1 + mu));
         e.sx = mu;
-        e.sy = st * cp;
-        e.sz = st * sp;
-        if (e.sx == (R)0) e.sx = (R)1e-10;  // :132-137
-        if (e.sy == (R)0) e.sy = (R)1e-10;
-        if (e.sz == (R)0) e.sz = (R)1e-10;
-        nb = bisect(S.cdf_f, S.nB, u_b);
+        nb = guided_index(S.cdf_f, S.guide_f, S.nB, u_b);
         g = (S.nQ > 1) ? bisect(S.probg + ((size_t)S.row * S.nB + nb) * S.nQ, S.nQ, u_g) : 0;
         const DLevel<R> &L0 = S.lev[0];
-        Pi = L0.P[((k - 1) * L0.jm + (j - 1)) * L0.im + (i - 1)];
+        Pi = L0.P[cell_index(i, j, k, L0.nbi, L0.nbj)];
+        e.xp = S.xc[i];
     } else {
         // Lambertian: theta = acos(1 - 2u)/2 (+pi/2 on the east wall)
         // (emiss_angS, :1093-1102), i.e. cos = sqrt(1-u) / -sqrt(u).
         const int bound = kind - 1;
-        R st;
         if (bound == 0) {
             e.sx = RT<R>::sqrt_((R)1 - u_mu);
             st = RT<R>::sqrt_(u_mu);
@@ -225,84 +296,88 @@ __device__ __forceinline__ bool emit_bundle(Emitted<R> &e, const DSolve<R> &S, i
             e.sx = -RT<R>::sqrt_(u_mu);
             st = RT<R>::sqrt_((R)1 - u_mu);
         }
-        e.sy = st * cp;
-        e.sz = st * sp;
+        nb = guided_index(S.cdf_s, S.guide_s, S.nB, u_b);
+        g = (S.nQ > 1) ? bisect(S.probq, S.nQ, u_g) : 0;
+        Pi = S.Pw0[bound][(k - 1) * S.jmax + (j - 1)];
+        ic = (bound == 0) ? 1 : S.imax;
+        e.xp = (bound == 0) ? (R)0 : S.Lx;
+    }
+    e.sy = st * cp;
+    e.sz = st * sp;
+    if (kind == 0) {
+        if (e.sx == (R)0) e.sx = (R)1e-10;  // :132-137
+        if (e.sy == (R)0) e.sy = (R)1e-10;
+        if (e.sz == (R)0) e.sz = (R)1e-10;
+    } else {
+        const int bound = kind - 1;
         if (RT<R>::fabs_(e.sx) <= (R)1e-10) e.sx = (R)(1 - 2 * bound) * (R)1e-10;  // :1395-1400
         if (RT<R>::fabs_(e.sy) <= (R)1e-10) e.sy = (R)((e.sy > (R)0) - (e.sy <= (R)0)) * (R)1e-10;
         if (RT<R>::fabs_(e.sz) <= (R)1e-10) e.sz = (R)((e.sz > (R)0) - (e.sz <= (R)0)) * (R)1e-10;
-        nb = bisect(S.cdf_s, S.nB, u_b);
-        g = (S.nQ > 1) ? bisect(S.probq, S.nQ, u_g) : 0;
-        Pi = S.Pw0[bound][(k - 1) * S.jmax + (j - 1)];
     }
     e.nbg = nb | (g << 20);
-    e.isx = (R)1 / e.sx;
-    e.isy = (R)1 / e.sy;
-    e.isz = (R)1 / e.sz;
-    // OERM weights (:180-186 fluid, :1421-1424 walls)
-    const R *kcol = S.kt + ((size_t)nb * S.nQ + g) * S.nT;
-    const R *ibcol = S.Ibt + (size_t)nb * S.nT;
-    const R Ib_i = tab_lerp(ibcol, S.nT, Pi);
-    const R Ib_m = tab_lerp(ibcol, S.nT, S.Pm);
-    if (!(Ib_i > (R)0) || !(Ib_m > (R)0)) return false;
+    int jc = j, kc = k;
+    if (kind != 0) {
+        // cell shift when the start point lies on a face (:1429-1441)
+        const DLevel<R> &G = S.lev[0];
+        const bool fx = e.sx < (R)0, fy = e.sy < (R)0, fz = e.sz < (R)0;
+        if (fx && e.xp == G.xu[ic - 1]) ic = ic - 1;
+        if (fy && e.yp == G.yu[jc - 1]) jc = jc - 1;
+        if (fz && e.zp == G.zu[kc - 1]) kc = kc - 1;
+        if (!fx && e.xp == G.xu[ic]) ic = ic + 1;
+        if (!fy && e.yp == G.yu[jc]) jc = jc + 1;
+        if (!fz && e.zp == G.zu[kc]) kc = kc + 1;
+    }
+    e.ij = ic | (jc << 16);
+    e.kk = kc | (kind << 16);
+    // OERM weights
+    const KIRow<R> row = S.ki[((size_t)nb * S.nQ + g) * S.nT + (Pi >> 8)];
+    const R fr = coord_frac<R>(Pi);
+    const R Ib_i = row.ib0 * ((R)1 - fr) + row.ib1 * fr;
+    if (!(Ib_i > (R)0)) return false;
     e.invTi4 = (R)1 / Ib_i;
     if (kind == 0) {
-        const R k_i = tab_lerp(kcol, S.nT, Pi);
-        const R k_m = tab_lerp(kcol, S.nT, S.Pm);
-        if (!(k_m > (R)0)) return false;
-        e.ratioI = ((((R)1 / e.invTi4) / Ib_m) * k_i) / k_m;
+        const R k_i = row.k0 * ((R)1 - fr) + row.k1 * fr;
+        const R den = S.den_f[(size_t)nb * S.nQ + g];
+        if (!(den > (R)0)) return false;
+        e.ratioI = (Ib_i * k_i) / den;
     } else {
-        e.ratioI = ((R)1 / e.invTi4) / Ib_m;
+        const R den = S.ibm[nb];
+        if (!(den > (R)0)) return false;
+        e.ratioI = Ib_i / den;
     }
     return true;
 }
 
-// Position, cell and weights of an emitted bundle at its start point.
+// Ray state of an emitted bundle.
 template <typename R>
-__device__ __forceinline__ void place_bundle(Ray<R> &r, const DSolve<R> &S, const Emitted<R> &e, int kind, int i,
-                                             int j, int k) {
+__device__ __forceinline__ void place_bundle(Ray<R> &r, const DSolve<R> &S, const Emitted<R> &e) {
+    r.xp = e.xp;
+    r.yp = e.yp;
+    r.zp = e.zp;
     r.sx = e.sx;
     r.sy = e.sy;
     r.sz = e.sz;
-    r.isx = e.isx;
-    r.isy = e.isy;
-    r.isz = e.isz;
+    r.isx = (R)1 / e.sx;
+    r.isy = (R)1 / e.sy;
+    r.isz = (R)1 / e.sz;
     r.ratioI = e.ratioI;
     r.invTi4 = e.invTi4;
     const int nb = e.nbg & 0xfffff, g = e.nbg >> 20;
     r.nb = nb;
-    r.kcol = S.kt + ((size_t)nb * S.nQ + g) * S.nT;
-    r.ibcol = S.Ibt + (size_t)nb * S.nT;
+    r.kicol = S.ki + ((size_t)nb * S.nQ + g) * S.nT;
     r.fx = r.sx < (R)0;
     r.fy = r.sy < (R)0;
     r.fz = r.sz < (R)0;
+    r.ic = e.ij & 0xffff;
+    r.jc = e.ij >> 16;
+    r.kc = e.kk & 0xffff;
+    const int kind = e.kk >> 16;
     r.lev = 0;
     r.counter = 0;
     r.tra = (R)1;
     r.De = 0.0;
-    r.jc = j;
-    r.kc = k;
-    r.yp = S.yc[j];
-    r.zp = S.zc[k];
-    if (kind == 0) {
-        r.ic = i;
-        r.xp = S.xc[i];
-        r.Ibmax = S.Ibmax_f;
-        r.tol = S.toll;
-    } else {
-        const int bound = kind - 1;
-        r.ic = (bound == 0) ? 1 : S.imax;
-        r.xp = (bound == 0) ? (R)0 : S.Lx;
-        r.Ibmax = bound == 0 ? S.Ibmax_w0 : S.Ibmax_w1;
-        r.tol = S.tollS;
-        // cell shift when the start point lies on a face (:1429-1441)
-        const DLevel<R> &G = S.lev[0];
-        if (r.fx && r.xp == G.xu[r.ic - 1]) r.ic = r.ic - 1;
-        if (r.fy && r.yp == G.yu[r.jc - 1]) r.jc = r.jc - 1;
-        if (r.fz && r.zp == G.zu[r.kc - 1]) r.kc = r.kc - 1;
-        if (!r.fx && r.xp == G.xu[r.ic]) r.ic = r.ic + 1;
-        if (!r.fy && r.yp == G.yu[r.jc]) r.jc = r.jc + 1;
-        if (!r.fz && r.zp == G.zu[r.kc]) r.kc = r.kc + 1;
-    }
+    r.Ibmax = kind == 0 ? S.Ibmax_f : kind == 1 ? S.Ibmax_w0 : S.Ibmax_w1;
+    r.tol = kind == 0 ? S.toll : S.tollS;
 }
 
 // Deposit the remaining energy on a black wall emitting Ib_wall
@@ -336,7 +411,10 @@ __device__ __forceinline__ void hit_wall(Ray<R> &r, const DSolve<R> &S, const DL
         if (w <= RC_EAST) idx = (r.kc - 1) * L.jm + (r.jc - 1);
         else if (w <= RC_NORTH) idx = (r.kc - 1) * L.im + (r.ic - 1);
         else idx = (r.jc - 1) * L.im + (r.ic - 1);
-        wall_deposit(r, tab_lerp(r.ibcol, S.nT, L.Pw[w][idx]));
+        const int q = L.Pw[w][idx];
+        const KIRow<R> row = r.kicol[q >> 8];
+        const R fr = coord_frac<R>(q);
+        wall_deposit(r, row.ib0 * ((R)1 - fr) + row.ib1 * fr);
     } else if (t == 3) {  // specular
         switch (w) {
             case RC_WEST: r.xp = (R)0; r.sx = -r.sx; r.isx = -r.isx; r.ic = 1; r.fx = r.sx < (R)0; break;
@@ -358,15 +436,14 @@ __device__ __forceinline__ void march_step(Ray<R> &r, const DSolve<R> &S, const 
     const R fxu = L.xu[r.ic - r.fx];
     const R fyu = L.yu[r.jc - r.fy];
     const R fzu = L.zu[r.kc - r.fz];
-    const R p = __ldg(&L.P[((r.kc - 1) * L.jm + (r.jc - 1)) * L.im + (r.ic - 1)]);
+    const int q = __ldg(&L.P[cell_index(r.ic, r.jc, r.kc, L.nbi, L.nbj)]);
+    const KIRow<R> row = load_row(r.kicol + (q >> 8));
     const R dsx = (fxu - r.xp) * r.isx;
     const R dsy = (fyu - r.yp) * r.isy;
     const R dsz = (fzu - r.zp) * r.isz;
-    const int i0 = (int)p;
-    const int i1 = min(i0 + 1, S.nT - 1);
-    const R a = p - (R)i0;
-    const R absco = lerp_at(r.kcol, i0, i1, a);
-    const R blackpow = lerp_at(r.ibcol, i0, i1, a);
+    const R a = coord_frac<R>(q);
+    const R absco = row.k0 * ((R)1 - a) + row.k1 * a;
+    const R blackpow = row.ib0 * ((R)1 - a) + row.ib1 * a;
     R ds = dsx;
     if (ds > dsy) ds = dsy;
     if (ds > dsz) ds = dsz;
@@ -388,21 +465,25 @@ __device__ __forceinline__ void march_step(Ray<R> &r, const DSolve<R> &S, const 
         r.De -= (double)c2;
         r.tra = (R)0;
     }
-    int axis;
-    if (dsx < dsy) axis = (dsx < dsz) ? 0 : 2;
-    else axis = (dsy < dsz) ? 1 : 2;
-    int w = -1;
+    // crossed axis (ties: x only if strictly smallest, :375-377, 524)
+    const int axis = (dsx < dsy) ? ((dsx < dsz) ? 0 : 2) : ((dsy < dsz) ? 1 : 2);
+    const int f = axis == 0 ? r.fx : (axis == 1 ? r.fy : r.fz);
+    const int dlt = f ? -1 : 1;
+    int nidx, lim;
     if (axis == 0) {
-        if (r.fx) { if (--r.ic == 0) w = RC_WEST; }
-        else { if (++r.ic == L.im + 1) w = RC_EAST; }
+        r.ic += dlt;
+        nidx = r.ic;
+        lim = L.im + 1;
     } else if (axis == 1) {
-        if (r.fy) { if (--r.jc == 0) w = RC_SOUTH; }
-        else { if (++r.jc == L.jm + 1) w = RC_NORTH; }
+        r.jc += dlt;
+        nidx = r.jc;
+        lim = L.jm + 1;
     } else {
-        if (r.fz) { if (--r.kc == 0) w = RC_BOT; }
-        else { if (++r.kc == L.km + 1) w = RC_TOP; }
+        r.kc += dlt;
+        nidx = r.kc;
+        lim = L.km + 1;
     }
-    if (w >= 0) hit_wall(r, S, L, w);
+    if (nidx == 0 || nidx == lim) hit_wall(r, S, L, 2 * axis + (nidx != 0));
     r.counter += 1;
 }
 
@@ -423,6 +504,13 @@ __device__ __forceinline__ bool level_advance(Ray<R> &r, const DSolve<R> &S) {
     return true;
 }
 
+// n / d for a divisor fixed per solve: with M = floor((2^64 - 1)/d) + 1,
+// floor(n M / 2^64) = floor(n / d) whenever n d < 2^64 (the host checks the
+// bound when it builds the descriptor); M = 0 encodes d = 1.
+__device__ __forceinline__ unsigned long long fdiv(unsigned long long n, unsigned long long M) {
+    return M ? __umul64hi(n, M) : n;
+}
+
 // Decoded work item: item = ((cell*nVar + v)*nchunk + q); the wall items
 // follow the fluid items.  kind = -1 marks an item past the end.
 struct ItemId {
@@ -435,30 +523,31 @@ __device__ __forceinline__ ItemId decode_item(const DSolve<R> &S, long long item
     d.kind = -1;
     d.i = d.j = d.k = d.v = d.h0 = 0;
     if (item >= S.n_items) return d;
-    long long it = item;
+    unsigned long long it = (unsigned long long)item;
     int kind = 0;
-    if (it >= S.n_fluid_items) {
-        it -= S.n_fluid_items;
+    if (item >= S.n_fluid_items) {
+        it -= (unsigned long long)S.n_fluid_items;
         kind = 1;
     }
-    const int q = (int)(it % S.nchunk);
-    const long long t = it / S.nchunk;
-    d.v = (int)(t % S.nVar);
-    const long long c = t / S.nVar;
+    const unsigned long long t = fdiv(it, S.mg_nchunk);
+    const int q = (int)(it - t * (unsigned long long)S.nchunk);
+    const unsigned long long c = fdiv(t, S.mg_nvar);
+    d.v = (int)(t - c * (unsigned long long)S.nVar);
     d.h0 = q * S.rpt;
     if (kind == 0) {
-        d.i = (int)(c % S.imax) + 1;
-        const long long cj = c / S.imax;
-        d.j = (int)(cj % S.jmax) + 1;
-        d.k = (int)(cj / S.jmax) + S.kfirst;
+        const unsigned long long cj = fdiv(c, S.mg_imax);
+        d.i = (int)(c - cj * (unsigned long long)S.imax) + 1;
+        const unsigned long long ck = fdiv(cj, S.mg_jmax);
+        d.j = (int)(cj - ck * (unsigned long long)S.jmax) + 1;
+        d.k = (int)ck + S.kfirst;
         d.kind = 0;
     } else {
-        const long long nwc = (long long)S.jmax * S.kloc;
-        const int slot = (int)(c / nwc);
-        const long long wc = c % nwc;
-        d.j = (int)(wc % S.jmax) + 1;
-        d.k = (int)(wc / S.jmax) + S.kfirst;
-        d.kind = 1 + S.wall_id[slot];
+        const unsigned long long slot = fdiv(c, S.mg_nwc);
+        const unsigned long long wc = c - slot * S.nwc;
+        const unsigned long long kw = fdiv(wc, S.mg_jmax);
+        d.j = (int)(wc - kw * (unsigned long long)S.jmax) + 1;
+        d.k = (int)kw + S.kfirst;
+        d.kind = 1 + S.wall_id[(int)slot];
     }
     return d;
 }

@@ -3,6 +3,7 @@
 // the tally.  Included once, by rc_solver.cu.
 #pragma once
 #include "rc_device.cuh"
+#include "rc_march.cuh"
 
 namespace rc {
 
@@ -96,7 +97,20 @@ __global__ void k_setup1(DScalars *sc, R *Tnb, const R *kP, int nT, int grey, fl
     const R inv_dT = (R)1 / (Tnb[1] - Tnb[0]);
     sc->T0 = (double)T0;
     sc->inv_dT = (double)inv_dT;
-    sc->Pm = (double)table_coord(Tmax, T0, inv_dT, nT);
+    sc->Pm = table_coord(Tmax, T0, inv_dT, nT);
+}
+
+// Copy the run-time values of a solve into its descriptor (after k_setup1,
+// before the march).
+template <typename R>
+__global__ void k_patch_desc(DSolve<R> *d, const DScalars *sc) {
+    if (threadIdx.x == 0 && blockIdx.x == 0) {
+        d->Pm = sc->Pm;
+        d->Ibmax_f = (R)sc->Ibmax_f;
+        d->Ibmax_w0 = (R)sc->Ibmax_w[0];
+        d->Ibmax_w1 = (R)sc->Ibmax_w[1];
+        d->row = sc->row;
+    }
 }
 
 __global__ void k_init_scalars(DScalars *sc) {
@@ -106,6 +120,22 @@ __global__ void k_init_scalars(DScalars *sc) {
         z.tmax_bits = 0u;
         z.tmin_bits = 0x7f800000u;
         *sc = z;
+    }
+}
+
+// Interleaved k / I_b rows {k[t], Ib[t], k[t+1], Ib[t+1]} (last row repeated).
+template <typename R>
+__global__ void k_build_ki(KIRow<R> *ki, const R *kt, const R *Ibt, int nB, int nQ, int nT) {
+    const int n = nB * nQ * nT;
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += gridDim.x * blockDim.x) {
+        const int t = e % nT, bg = e / nT, nb = bg / nQ;
+        const int t1 = min(t + 1, nT - 1);
+        KIRow<R> r;
+        r.k0 = kt[(size_t)bg * nT + t];
+        r.k1 = kt[(size_t)bg * nT + t1];
+        r.ib0 = Ibt[(size_t)nb * nT + t];
+        r.ib1 = Ibt[(size_t)nb * nT + t1];
+        ki[e] = r;
     }
 }
 
@@ -133,17 +163,46 @@ __device__ void planck_cdf_row(R *out, const R *Ibt, const R *wvl, const R *wvr,
     for (int b = 0; b < nB; ++b) out[b] = out[b] / last;
 }
 
-// Band CDF rows at the row nearest Tmax: fluid (copy, or the grey Planck
-// CDF) and walls (readS).
+// First index b with cdf[b] > x (n-1 if none).
 template <typename R>
-__global__ void k_setup2(const DScalars *sc, R *cdf_f, R *cdf_s, const R *prob, const R *Ibt, const R *wvl,
-                         const R *wvr, int nT, int nB, int grey, int walls) {
+__device__ int first_above(const R *cdf, int n, R x) {
+    int lo = 0, hi = n - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if (cdf[mid] > x) hi = mid;
+        else lo = mid + 1;
+    }
+    return lo;
+}
+
+// Per-solve sampling tables (one block): band CDF rows at the row nearest
+// Tmax -- fluid (copy, or the grey Planck CDF) and walls (readS,
+// read_tables.cpp:188-220) -- their guide tables, and the Tmax factors of
+// the OERM weights, I_b(Tmax) k_g(Tmax) per (band, g) and I_b(Tmax) per band.
+template <typename R>
+__global__ void k_setup2(const DScalars *sc, R *cdf_f, R *cdf_s, int *guide_f, int *guide_s, R *den_f, R *ibm,
+                         const R *prob, const R *Ibt, const R *kt, const R *wvl, const R *wvr, int nT, int nB,
+                         int nQ, int grey, int walls) {
     const int row = sc->row;
+    const int Pm = sc->Pm;
     if (!grey) {
         for (int b = threadIdx.x; b < nB; b += blockDim.x) cdf_f[b] = prob[(size_t)row * nB + b];
     }
     if (threadIdx.x == 0 && grey) planck_cdf_row(cdf_f, Ibt, wvl, wvr, nT, nB, row);
     if (threadIdx.x == 32 % blockDim.x && walls) planck_cdf_row(cdf_s, Ibt, wvl, wvr, nT, nB, row);
+    for (int e = threadIdx.x; e < nB * nQ; e += blockDim.x) {
+        const int nb = e / nQ, g = e % nQ;
+        const R Ib_m = tab_lerp(Ibt + (size_t)nb * nT, nT, Pm);
+        const R k_m = tab_lerp(kt + ((size_t)nb * nQ + g) * nT, nT, Pm);
+        den_f[e] = Ib_m * k_m;
+        if (g == 0) ibm[nb] = Ib_m;
+    }
+    __syncthreads();
+    for (int q = threadIdx.x; q < kGuide; q += blockDim.x) {
+        const R x = (R)q / (R)kGuide;
+        guide_f[q] = first_above(cdf_f, nB, x);
+        if (walls) guide_s[q] = first_above(cdf_s, nB, x);
+    }
 }
 
 // Texture-space trilinear sample of the float field with clamped indices
@@ -176,7 +235,8 @@ __device__ __forceinline__ float tex_sample(const float *T, int nx, int ny, int 
 // or the emission temperature of a wall at that level (:392-396, 468-472).
 struct LevelJob {
     void *dst;
-    int type;     // 0 cells, 1 + w: wall w
+    int type;     // 0 cells (4x4x4 bricks), 1 + w: wall w (linear)
+    int nbi, nbj; // bricks per x / y row (cells)
     int im, jm, km;
     int rx, ry, rz;   // fine cells per level cell (imax/im ...)
     int face;     // wall sampled at the face (1) or at the first cell (0)
@@ -200,7 +260,7 @@ __global__ void k_levels(const float *__restrict__ T, int imax, int jmax, int km
         while (jb + 1 < jobs.njobs && jobs.job[jb + 1].start <= e) ++jb;
         const LevelJob &J = jobs.job[jb];
         const long long l = e - J.start;
-        R *dst = (R *)J.dst;
+        uint16_t *dst = (uint16_t *)J.dst;
         const float rxf = (float)J.rx, ryf = (float)J.ry, rzf = (float)J.rz;
         if (J.type == 0) {
             const int ic = (int)(l % J.im) + 1;
@@ -210,7 +270,8 @@ __global__ void k_levels(const float *__restrict__ T, int imax, int jmax, int km
             const float t1 = ((float)ic - 0.5f) * rxf + 1.0f;
             const float t2 = ((float)jc - 0.5f) * ryf + 1.0f;
             const float t3 = ((float)kc - 0.5f) * rzf + 1.0f;
-            dst[l] = table_coord((R)tex_sample(T, nx, ny, nz, t1, t2, t3), T0, inv_dT, nT);
+            dst[cell_index(ic, jc, kc, J.nbi, J.nbj)] =
+                (uint16_t)table_coord((R)tex_sample(T, nx, ny, nz, t1, t2, t3), T0, inv_dT, nT);
         } else {
             const int w = J.type - 1;
             float x, y, z;
@@ -230,182 +291,9 @@ __global__ void k_levels(const float *__restrict__ T, int imax, int jmax, int km
                 y = ((float)jc - 0.5f) * ryf + 1.0f;
                 z = (w == RC_BOT) ? (J.face ? 1.0f : 1.5f) : (J.face ? (float)kmax + 1.0f : (float)kmax + 0.5f);
             }
-            dst[l] = table_coord((R)tex_sample(T, nx, ny, nz, x, y, z), T0, inv_dT, nT);
+            dst[l] = (uint16_t)table_coord((R)tex_sample(T, nx, ny, nz, x, y, z), T0, inv_dT, nT);
         }
     }
-}
-
-// ---------------------------------------------------------------------------
-// march: persistent warps over tiles of 32 work items
-// ---------------------------------------------------------------------------
-//
-// A work item is one chunk of rays_per_thread consecutive bundles of one
-// (cell, replicate).  A warp takes a tile of 32 items, i.e. a pool of
-// 32*rays_per_thread bundles:
-//   * the 32 items are decoded once, one per lane;
-//   * bundles are emitted in converged waves of 32 (all lanes run the
-//     Philox draws, direction, band/g bisection and OERM weights together)
-//     into a per-warp ring in shared memory, whenever the ring holds fewer
-//     than 32 bundles;
-//   * every lane traces one ray; when its ray ends it takes the next
-//     emitted bundle from the ring (warp ballot + prefix count), so lanes
-//     never wait for each other while the pool has bundles;
-//   * each bundle's FP64 tally goes to its own shared-memory slot; at the end
-//     of the tile the slots are summed in bundle order, so the result does
-//     not depend on which lane traced which bundle.
-
-struct MarchArgs {
-    const void *solves;          // DSolve<R>[nsolves]
-    const long long *tile_start; // [nsolves+1] exclusive prefix of tiles
-    int nsolves;
-    long long total_tiles;
-    unsigned long long *tile_counter;
-    int rpt_max;
-};
-
-template <typename R>
-struct WarpShared {
-    DSolve<R> sd;
-    ItemId items[kWarp];
-    Emitted<R> ring[kRing];
-};
-
-template <typename R>
-__device__ __forceinline__ void load_solve(DSolve<R> *dst, const DSolve<R> *src, int lane) {
-    const int *s = reinterpret_cast<const int *>(src);
-    int *d = reinterpret_cast<int *>(dst);
-    constexpr int nw = (int)(sizeof(DSolve<R>) / 4);
-    for (int w = lane; w < nw; w += kWarp) d[w] = s[w];
-    __syncwarp();
-    if (lane == 0) {
-        const DScalars *sc = dst->sc;
-        dst->Pm = (R)sc->Pm;
-        dst->Ibmax_f = (R)sc->Ibmax_f;
-        dst->Ibmax_w0 = (R)sc->Ibmax_w[0];
-        dst->Ibmax_w1 = (R)sc->Ibmax_w[1];
-        dst->row = sc->row;
-    }
-    __syncwarp();
-}
-
-// MINB: resident 256-thread blocks per SM the register allocation must
-// allow (2: up to 128 registers, 3: 80, 4: 64).
-template <typename R, int MINB>
-__global__ void __launch_bounds__(256, MINB) k_march(MarchArgs a) {
-    extern __shared__ __align__(16) unsigned char smem[];
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
-    WarpShared<R> *ws = reinterpret_cast<WarpShared<R> *>(smem) + warp;
-    const size_t wbytes = ((sizeof(WarpShared<R>) * nwarps) + 15) & ~(size_t)15;
-    double *slots = reinterpret_cast<double *>(smem + wbytes) + (size_t)warp * kWarp * a.rpt_max;
-    const DSolve<R> *solves = reinterpret_cast<const DSolve<R> *>(a.solves);
-    const unsigned lt = (1u << lane) - 1u;
-    int cur = -1;
-    for (;;) {
-        unsigned long long tile = 0;
-        if (lane == 0) tile = atomicAdd(a.tile_counter, 1ull);
-        tile = __shfl_sync(0xffffffffu, tile, 0);
-        if (tile >= (unsigned long long)a.total_tiles) break;
-        int lo = 0, hi = a.nsolves;
-        while (hi - lo > 1) {
-            const int mid = (lo + hi) >> 1;
-            if ((unsigned long long)a.tile_start[mid] <= tile) lo = mid;
-            else hi = mid;
-        }
-        if (lo != cur) {
-            load_solve(&ws->sd, solves + lo, lane);
-            cur = lo;
-        }
-        const DSolve<R> &S = ws->sd;
-        const long long item0 = (long long)(tile - (unsigned long long)a.tile_start[lo]) * kWarp;
-        const int rpt = S.rpt;
-        const int lrpt = __ffs(rpt) - 1;  // rpt is a power of two
-        const int pool = kWarp * rpt;
-        ws->items[lane] = decode_item(S, item0 + lane);
-        for (int b = lane; b < pool; b += kWarp) slots[b] = 0.0;
-        __syncwarp();
-        int next_b = 0, head = 0, count = 0;
-        bool active = false;
-        int myb = 0;
-        unsigned int nsteps = 0, nbund = 0;
-        Ray<R> r;
-        for (;;) {
-            if (count < kWarp && next_b < pool) {
-                // converged emission wave: one bundle per lane
-                const int b = next_b + lane;
-                Emitted<R> e;
-                bool ok = false;
-                if (b < pool) {
-                    const ItemId it = ws->items[b >> lrpt];
-                    const int h = it.h0 + (b & (rpt - 1));
-                    if (it.kind >= 0 && h < S.photmax) {
-                        nbund++;
-                        ok = emit_bundle(e, S, it.kind, it.i, it.j, it.k, it.v, h);
-                        e.b = b;
-                    }
-                }
-                const unsigned m = __ballot_sync(0xffffffffu, ok);
-                if (ok) ws->ring[(head + count + __popc(m & lt)) & (kRing - 1)] = e;
-                count += __popc(m);
-                next_b += kWarp;
-                __syncwarp();
-            }
-            const bool need = !active;
-            const unsigned m = __ballot_sync(0xffffffffu, need);
-            const int navail = min(count, __popc(m));
-            if (need) {
-                const int rank = __popc(m & lt);
-                if (rank < navail) {
-                    const Emitted<R> e = ws->ring[(head + rank) & (kRing - 1)];
-                    const ItemId it = ws->items[e.b >> lrpt];
-                    place_bundle(r, S, e, it.kind, it.i, it.j, it.k);
-                    myb = e.b;
-                    active = level_advance(r, S);
-                    if (!active) slots[myb] = r.De;
-                }
-            }
-            head = (head + navail) & (kRing - 1);
-            count -= navail;
-            if (!__any_sync(0xffffffffu, active) && count == 0 && next_b >= pool) break;
-            if (active) {
-                march_step(r, S, S.lev[r.lev]);
-                nsteps++;
-                bool done = !(r.tra > r.tol);
-                if (!done) done = !level_advance(r, S);
-                if (done) {
-                    slots[myb] = r.De;
-                    active = false;
-                }
-            }
-            __syncwarp();
-        }
-        __syncwarp();
-        // chunk sum of this lane's item, then group sums in item order
-        double s = 0.0;
-        for (int h = 0; h < rpt; ++h) s += slots[lane * rpt + h];
-        const int gs = S.gsize;
-        const int base = (lane / gs) * gs;
-        double g = 0.0;
-        for (int q = 0; q < gs; ++q) g += __shfl_sync(0xffffffffu, s, base + q);
-        const long long item = item0 + lane;
-        if (lane == base && item < S.n_items) S.partial[item / gs] = g;
-        // counters
-        unsigned long long st = nsteps, nb = nbund;
-        for (int o = 16; o > 0; o >>= 1) {
-            st += __shfl_xor_sync(0xffffffffu, st, o);
-            nb += __shfl_xor_sync(0xffffffffu, nb, o);
-        }
-        if (lane == 0) {
-            atomicAdd(&S.sc->steps, st);
-            atomicAdd(&S.sc->bundles, nb);
-        }
-        __syncwarp();
-    }
-}
-
-template <typename R>
-constexpr size_t march_smem_bytes(int block, int rpt_max) {
-    return ((((size_t)sizeof(WarpShared<R>) * (block / kWarp)) + 15) & ~(size_t)15) +
-           (size_t)(block / kWarp) * kWarp * rpt_max * sizeof(double);
 }
 
 // ---------------------------------------------------------------------------
@@ -469,7 +357,7 @@ __global__ void k_trace(const DSolve<R> *Sp, int n, const rc_bundle_id *ids, rc_
     if (t >= n) return;
     DSolve<R> S = *Sp;
     const DScalars *sc = S.sc;
-    S.Pm = (R)sc->Pm;
+    S.Pm = sc->Pm;
     S.Ibmax_f = (R)sc->Ibmax_f;
     S.Ibmax_w0 = (R)sc->Ibmax_w[0];
     S.Ibmax_w1 = (R)sc->Ibmax_w[1];
@@ -491,7 +379,7 @@ __global__ void k_trace(const DSolve<R> *Sp, int n, const rc_bundle_id *ids, rc_
     rec.sz = (float)e.sz;
     if (ok) {
         Ray<R> r;
-        place_bundle(r, S, e, id.kind, id.i, id.j, id.k);
+        place_bundle(r, S, e);
         bool active = level_advance(r, S);
         int ns = 0;
         while (active) {

@@ -1,0 +1,263 @@
+// rc_march.cuh -- the persistent march kernel (kernel_fluid + march_ray +
+// kernel_surface of src/montecarlo/mc_gpu_noint.cu, restructured for SIMT).
+#pragma once
+#include "rc_device.cuh"
+
+namespace rc {
+
+// ---------------------------------------------------------------------------
+// march: persistent warps over tiles of 32 work items
+// ---------------------------------------------------------------------------
+//
+// A work item is one chunk of rays_per_thread consecutive bundles of one
+// (cell, replicate).  A warp takes tiles of 32 items, i.e. pools of
+// 32*rays_per_thread bundles:
+//   * bundles are emitted in converged waves of 32 (all lanes decode their
+//     item and run the Philox draws, direction, band/g search and OERM
+//     weights together) into a per-warp ring in shared memory whenever the
+//     ring holds fewer than 32 bundles;
+//   * every lane traces one ray; the warp steps all its rays until at least
+//     kFeedIdle lanes are idle, then hands those lanes the next emitted
+//     bundles (warp ballot + prefix count);
+//   * two tiles can be in flight: once every bundle of a tile has been
+//     emitted, the warp fetches the next tile (of the same solve) and keeps
+//     emitting from it while the last rays of the previous tile finish, so
+//     long rays do not leave the other lanes idle at tile ends;
+//   * each bundle's FP64 tally goes to its own shared-memory slot; when a
+//     tile's last bundle has finished, its slots are summed in bundle
+//     order, so the result does not depend on which lane traced which
+//     bundle.
+// Shared memory per warp is the ring (64 emitted bundles) and two slot
+// arrays; everything else stays in L1-cached global memory, so that most of
+// the SM's 256 KB of L1/shared storage caches the temperature pyramid and
+// the k / I_b tables.
+
+struct MarchArgs {
+    const void *solves;          // DSolve<R>[nsolves] (run-time fields patched on the device)
+    const long long *tile_start; // [nsolves+1] exclusive prefix of tiles
+    int nsolves;
+    long long total_tiles;
+    unsigned long long *tile_counter;
+    int rpt_max;
+};
+
+template <typename R>
+struct WarpShared {
+    Emitted<R> ring[kRing];
+};
+
+// Index of the solve owning a global tile (tile_start is an exclusive prefix).
+__device__ __forceinline__ int solve_of_tile(const long long *tile_start, int nsolves, unsigned long long tile) {
+    int lo = 0, hi = nsolves;
+    while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if ((unsigned long long)tile_start[mid] <= tile) lo = mid;
+        else hi = mid;
+    }
+    return lo;
+}
+
+__device__ __forceinline__ void flush_counters(DScalars *sc, unsigned long long &nsteps, unsigned long long &nbund,
+                                               int lane) {
+    unsigned long long st = nsteps, nb = nbund;
+    for (int o = 16; o > 0; o >>= 1) {
+        st += __shfl_xor_sync(0xffffffffu, st, o);
+        nb += __shfl_xor_sync(0xffffffffu, nb, o);
+    }
+    if (lane == 0) {
+        atomicAdd(&sc->steps, st);
+        atomicAdd(&sc->bundles, nb);
+    }
+    nsteps = nbund = 0;
+}
+
+// MINB: resident 256-thread blocks per SM the register allocation must
+// allow (2: up to 128 registers, 3: 80, 4: 64).
+template <typename R, int MINB>
+__global__ void __launch_bounds__(256, MINB) k_march(MarchArgs a) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+    WarpShared<R> *ws = reinterpret_cast<WarpShared<R> *>(smem) + warp;
+    const size_t wbytes = ((sizeof(WarpShared<R>) * nwarps) + 15) & ~(size_t)15;
+    const int pool_max = kWarp * a.rpt_max;
+    double *slots0 = reinterpret_cast<double *>(smem + wbytes) + (size_t)warp * 2 * pool_max;
+    const DSolve<R> *solves = reinterpret_cast<const DSolve<R> *>(a.solves);
+    const unsigned lt = (1u << lane) - 1u;
+    const DSolve<R> *Sp = solves;
+
+    // warp-uniform state
+    int cur_solve = -1;
+    long long item0_0 = 0, item0_1 = 0;  // first item of the tile in each buffer
+    unsigned busy = 0u;     // bit p: buffer p holds a tile not yet reduced
+    unsigned emitted = 0u;  // bit p: every bundle of buffer p's tile emitted
+    int out0 = 0, out1 = 0; // emitted bundles of each buffer not finished yet
+    int epar = -1;          // buffer being emitted from
+    int next_b = 0, head = 0, count = 0;
+    bool drained = false;   // no more tiles
+    unsigned long long pending = ~0ull;  // fetched tile waiting for a solve switch
+    // lane state
+    bool active = false;
+    int myb = 0, mypar = 0;
+    unsigned long long nsteps = 0, nbund = 0;
+    Ray<R> r;
+
+    for (;;) {
+        // ---- fetch the next tile into a free buffer
+        if (!drained && (epar < 0 || ((emitted >> epar) & 1u))) {
+            const int fpar = (epar < 0) ? 0 : (epar ^ 1);
+            if (!((busy >> fpar) & 1u)) {
+                unsigned long long tile = pending;
+                if (tile == ~0ull) {
+                    if (lane == 0) tile = atomicAdd(a.tile_counter, 1ull);
+                    tile = __shfl_sync(0xffffffffu, tile, 0);
+                }
+                if (tile >= (unsigned long long)a.total_tiles) {
+                    drained = true;
+                    pending = ~0ull;
+                } else {
+                    const int so = solve_of_tile(a.tile_start, a.nsolves, tile);
+                    if (so != cur_solve && busy) {
+                        pending = tile;  // switch solves only once both buffers are reduced
+                    } else {
+                        pending = ~0ull;
+                        if (so != cur_solve) {
+                            if (cur_solve >= 0) flush_counters(Sp->sc, nsteps, nbund, lane);
+                            Sp = solves + so;
+                            cur_solve = so;
+                        }
+                        const long long i0 = (long long)(tile - (unsigned long long)a.tile_start[so]) * kWarp;
+                        if (fpar) item0_1 = i0;
+                        else item0_0 = i0;
+                        double *sl = slots0 + fpar * pool_max;
+                        for (int b = lane; b < kWarp * Sp->rpt; b += kWarp) sl[b] = 0.0;
+                        busy |= 1u << fpar;
+                        emitted &= ~(1u << fpar);
+                        if (fpar) out1 = 0;
+                        else out0 = 0;
+                        epar = fpar;
+                        next_b = 0;
+                        __syncwarp();
+                    }
+                }
+            }
+        }
+        const DSolve<R> &S = *Sp;
+        const int rpt = S.rpt;
+        const int lrpt = __ffs(rpt) - 1;  // rpt is a power of two
+        const int pool = kWarp * rpt;
+        // ---- converged emission wave: one bundle per lane
+        if (count < kWarp && epar >= 0 && !((emitted >> epar) & 1u)) {
+            const int b = next_b + lane;
+            Emitted<R> e;
+            bool ok = false;
+            if (b < pool) {
+                const ItemId it = decode_item(S, (epar ? item0_1 : item0_0) + (b >> lrpt));
+                const int h = it.h0 + (b & (rpt - 1));
+                if (it.kind >= 0 && h < S.photmax) {
+                    nbund++;
+                    ok = emit_bundle(e, S, it.kind, it.i, it.j, it.k, it.v, h);
+                    e.b = b | (epar << 16);
+                }
+            }
+            const unsigned m = __ballot_sync(0xffffffffu, ok);
+            if (ok) ws->ring[(head + count + __popc(m & lt)) & (kRing - 1)] = e;
+            count += __popc(m);
+            if (epar) out1 += __popc(m);
+            else out0 += __popc(m);
+            next_b += kWarp;
+            if (next_b >= pool) emitted |= 1u << epar;
+            __syncwarp();
+        }
+        // ---- idle lanes take emitted bundles
+        {
+            const bool need = !active;
+            const unsigned m = __ballot_sync(0xffffffffu, need);
+            const int navail = min(count, __popc(m));
+            bool fin = false;
+            if (need) {
+                const int rank = __popc(m & lt);
+                if (rank < navail) {
+                    const Emitted<R> &e = ws->ring[(head + rank) & (kRing - 1)];
+                    place_bundle(r, S, e);
+                    myb = e.b & 0xffff;
+                    mypar = e.b >> 16;
+                    active = level_advance(r, S);
+                    if (!active) {
+                        slots0[mypar * pool_max + myb] = r.De;
+                        fin = true;
+                    }
+                }
+            }
+            head = (head + navail) & (kRing - 1);
+            count -= navail;
+            const unsigned f1 = __ballot_sync(0xffffffffu, fin && mypar == 1);
+            const unsigned f0 = __ballot_sync(0xffffffffu, fin && mypar == 0);
+            out0 -= __popc(f0);
+            out1 -= __popc(f1);
+            __syncwarp();
+        }
+        // ---- step every active ray; stay in this loop until enough lanes
+        //      are idle to be worth handing out bundles (or a tile can be
+        //      reduced, or every lane is idle)
+        {
+            const bool can_feed =
+                count > 0 || (epar >= 0 && !((emitted >> epar) & 1u)) ||
+                (!drained && (epar < 0 || (((emitted >> epar) & 1u) && !((busy >> (epar ^ 1)) & 1u))));
+            for (;;) {
+                bool fin = false;
+                if (active) {
+                    march_step(r, S, S.lev[r.lev]);
+                    nsteps++;
+                    bool done = !(r.tra > r.tol);
+                    if (!done) done = !level_advance(r, S);
+                    if (done) {
+                        slots0[mypar * pool_max + myb] = r.De;
+                        active = false;
+                        fin = true;
+                    }
+                }
+                const unsigned fm = __ballot_sync(0xffffffffu, fin);
+                if (fm) {
+                    const int n1 = __popc(__ballot_sync(0xffffffffu, fin && mypar == 1));
+                    out1 -= n1;
+                    out0 -= __popc(fm) - n1;
+                }
+                const int nidle = __popc(__ballot_sync(0xffffffffu, !active));
+                if (nidle == kWarp) break;
+                if (nidle >= kFeedIdle && can_feed) break;
+                if (fm && ((((busy & emitted) & 1u) && out0 == 0) || (((busy & emitted) & 2u) && out1 == 0))) break;
+            }
+        }
+        // ---- reduce finished tiles: chunk sums in bundle order, group sums
+        //      in item order
+#pragma unroll
+        for (int par = 0; par < 2; ++par) {
+            const int outp = par ? out1 : out0;
+            if (((busy & emitted) >> par) & 1u && outp == 0) {
+                __syncwarp();
+                const double *sl = slots0 + par * pool_max;
+                double s = 0.0;
+                for (int h = 0; h < rpt; ++h) s += sl[lane * rpt + h];
+                const int gs = S.gsize;
+                const int base = (lane / gs) * gs;
+                double g = 0.0;
+                for (int q = 0; q < gs; ++q) g += __shfl_sync(0xffffffffu, s, base + q);
+                const long long item = (par ? item0_1 : item0_0) + lane;
+                if (lane == base && item < S.n_items) S.partial[item / gs] = g;
+                busy &= ~(1u << par);
+                if (epar == par) epar = -1;
+                __syncwarp();
+            }
+        }
+        if (drained && !busy) break;
+    }
+    if (cur_solve >= 0) flush_counters(Sp->sc, nsteps, nbund, lane);
+}
+
+template <typename R>
+constexpr size_t march_smem_bytes(int block, int rpt_max) {
+    return ((((size_t)sizeof(WarpShared<R>) * (block / kWarp)) + 15) & ~(size_t)15) +
+           (size_t)(block / kWarp) * 2 * kWarp * rpt_max * sizeof(double);
+}
+
+}  // namespace rc

@@ -146,10 +146,12 @@ namespace {
 
 template <typename R>
 struct Slot : SlotCommon {
-    std::vector<R *> d_levT;
-    R *d_lw[RC_MAX_LEVELS][6] = {};
-    R *d_Tw0[2] = {nullptr, nullptr};
-    R *d_cdf_f = nullptr, *d_cdf_s = nullptr;
+    std::vector<uint16_t *> d_levT;
+    uint16_t *d_lw[RC_MAX_LEVELS][6] = {};
+    uint16_t *d_Tw0[2] = {nullptr, nullptr};
+    KIRow<R> *d_ki_grey = nullptr;
+    R *d_cdf_f = nullptr, *d_cdf_s = nullptr, *d_den_f = nullptr, *d_ibm = nullptr;
+    int *d_guide_f = nullptr, *d_guide_s = nullptr;
     R *d_Tnb_grey = nullptr, *d_Ibt_grey = nullptr;
     DSolve<R> *d_desc = nullptr, *h_desc = nullptr;
     LevelJobs jobs;
@@ -162,6 +164,7 @@ struct Impl : ImplBase {
     R *d_xc = nullptr, *d_yc = nullptr, *d_zc = nullptr;
     R *d_kt = nullptr, *d_Ibt = nullptr, *d_probg = nullptr, *d_prob = nullptr, *d_probq = nullptr;
     R *d_Ibw = nullptr, *d_Tnb = nullptr, *d_kP = nullptr, *d_wvl = nullptr, *d_wvr = nullptr, *d_wvc = nullptr;
+    KIRow<R> *d_ki = nullptr;
     int nT = 0, nB = 0, nQ = 0;
     std::vector<Slot<R>> slots;
     int smem_opt_in = 0;
@@ -191,6 +194,7 @@ struct Impl : ImplBase {
         dfree(d_wvl);
         dfree(d_wvr);
         dfree(d_wvc);
+        dfree(d_ki);
     }
 
     void release() {
@@ -223,8 +227,13 @@ struct Impl : ImplBase {
                 for (int w = 0; w < 6; ++w) dfree(s.d_lw[l][w]);
             dfree(s.d_Tw0[0]);
             dfree(s.d_Tw0[1]);
+            dfree(s.d_ki_grey);
             dfree(s.d_cdf_f);
             dfree(s.d_cdf_s);
+            dfree(s.d_den_f);
+            dfree(s.d_ibm);
+            dfree(s.d_guide_f);
+            dfree(s.d_guide_s);
             dfree(s.d_Tnb_grey);
             dfree(s.d_Ibt_grey);
             dfree(s.d_desc);
@@ -319,6 +328,8 @@ struct Impl : ImplBase {
                 LevelJob &jb = J.job[J.njobs++];
                 jb.dst = dst;
                 jb.type = type;
+                jb.nbi = (p.maxi[l] + 3) / 4;
+                jb.nbj = (p.maxj[l] + 3) / 4;
                 jb.im = p.maxi[l];
                 jb.jm = p.maxj[l];
                 jb.km = p.maxk[l];
@@ -332,7 +343,9 @@ struct Impl : ImplBase {
             };
             for (int l = 0; l < nl; ++l) {
                 const long long n = (long long)p.maxi[l] * p.maxj[l] * p.maxk[l];
-                RC_CK(cudaMalloc((void **)&s.d_levT[l], n * sizeof(R)));
+                const long long nbr = (long long)((p.maxi[l] + 3) / 4) * ((p.maxj[l] + 3) / 4) * ((p.maxk[l] + 3) / 4);
+                RC_CK(cudaMalloc((void **)&s.d_levT[l], nbr * 64 * sizeof(uint16_t)));
+                RC_CK(cudaMemset(s.d_levT[l], 0, nbr * 64 * sizeof(uint16_t)));
                 add_job(s.d_levT[l], 0, l, 0, n);
                 for (int w = 0; w < 6; ++w) {
                     const int t = c->wt[w];
@@ -341,7 +354,7 @@ struct Impl : ImplBase {
                     if (w <= RC_EAST) n2 = (long long)p.maxj[l] * p.maxk[l];
                     else if (w <= RC_NORTH) n2 = (long long)p.maxi[l] * p.maxk[l];
                     else n2 = (long long)p.maxi[l] * p.maxj[l];
-                    RC_CK(cudaMalloc((void **)&s.d_lw[l][w], n2 * sizeof(R)));
+                    RC_CK(cudaMalloc((void **)&s.d_lw[l][w], n2 * sizeof(uint16_t)));
                     add_job(s.d_lw[l][w], 1 + w, l, t == WT_BLACK_FACE ? 1 : 0, n2);
                 }
             }
@@ -349,15 +362,22 @@ struct Impl : ImplBase {
             // wall kernel (kernel_surface :1359-1366)
             for (int b = 0; b < 2; ++b) {
                 const long long n2 = (long long)p.jmax * p.kmax;
-                RC_CK(cudaMalloc((void **)&s.d_Tw0[b], n2 * sizeof(R)));
+                RC_CK(cudaMalloc((void **)&s.d_Tw0[b], n2 * sizeof(uint16_t)));
                 add_job(s.d_Tw0[b], 1 + b, 0, 1, n2);
             }
             const int nBmax = p.grey ? p.grey_nB : p.nB;
             RC_CK(cudaMalloc((void **)&s.d_cdf_f, nBmax * sizeof(R)));
             RC_CK(cudaMalloc((void **)&s.d_cdf_s, nBmax * sizeof(R)));
+            const int nQmax = p.grey ? 1 : p.nQ;
+            RC_CK(cudaMalloc((void **)&s.d_den_f, (size_t)nBmax * nQmax * sizeof(R)));
+            RC_CK(cudaMalloc((void **)&s.d_ibm, nBmax * sizeof(R)));
+            RC_CK(cudaMalloc((void **)&s.d_guide_f, kGuide * sizeof(int)));
+            RC_CK(cudaMalloc((void **)&s.d_guide_s, kGuide * sizeof(int)));
+            RC_CK(cudaMemset(s.d_guide_s, 0, kGuide * sizeof(int)));
             if (p.grey) {
                 RC_CK(cudaMalloc((void **)&s.d_Tnb_grey, p.grey_nT * sizeof(R)));
                 RC_CK(cudaMalloc((void **)&s.d_Ibt_grey, (size_t)p.grey_nT * p.grey_nB * sizeof(R)));
+                RC_CK(cudaMalloc((void **)&s.d_ki_grey, (size_t)p.grey_nT * p.grey_nB * sizeof(KIRow<R>)));
             }
         }
         cudaDeviceProp prop;
@@ -414,6 +434,17 @@ struct Impl : ImplBase {
             return set_err(err_, RC_E_INVALID, "table dimensions differ from params nT/nB/nQ");
         if (t.nT < 2 || !(t.Tnb[1] > t.Tnb[0]))
             return set_err(err_, RC_E_INVALID, "table temperatures must be increasing");
+        if (t.nT > 256) return set_err(err_, RC_E_INVALID, "at most 256 table temperatures");
+        for (int i = 0; i < t.nT; ++i) {
+            // the band search assumes non-decreasing cumulative probabilities
+            for (int b = 1; b < t.nB; ++b)
+                if (t.prob[(size_t)i * t.nB + b] < t.prob[(size_t)i * t.nB + b - 1])
+                    return set_err(err_, RC_E_INVALID, "band cumulative probability decreases (prob_new2)");
+            for (int b = 0; b < t.nB; ++b)
+                for (int g = 1; g < t.nQ; ++g)
+                    if (t.probg[((size_t)i * t.nB + b) * t.nQ + g] < t.probg[((size_t)i * t.nB + b) * t.nQ + g - 1])
+                        return set_err(err_, RC_E_INVALID, "g cumulative probability decreases (prob_new2)");
+        }
         for (int i = 2; i < t.nT; ++i) {
             // the lookups assume uniform spacing (pos = (T - T0)/dT)
             const double d0 = t.Tnb[1] - t.Tnb[0], di = t.Tnb[i] - t.Tnb[i - 1];
@@ -461,6 +492,20 @@ struct Impl : ImplBase {
         if (!rc) rc = upload(d_wvr, t.wvr, err_);
         if (!rc) rc = upload(d_wvc, t.wvc, err_);
         if (rc) return rc;
+        // interleaved rows {k[t], Ib[t], k[t+1], Ib[t+1]} for the march
+        std::vector<KIRow<R>> ki((size_t)nB * nQ * nT);
+        for (int b = 0; b < nB; ++b)
+            for (int g = 0; g < nQ; ++g)
+                for (int i = 0; i < nT; ++i) {
+                    const int i1 = std::min(i + 1, nT - 1);
+                    KIRow<R> &r = ki[((size_t)b * nQ + g) * nT + i];
+                    r.k0 = (R)kt[((size_t)b * nQ + g) * nT + i];
+                    r.k1 = (R)kt[((size_t)b * nQ + g) * nT + i1];
+                    r.ib0 = (R)Ibt[(size_t)b * nT + i];
+                    r.ib1 = (R)Ibt[(size_t)b * nT + i1];
+                }
+        RC_CK(cudaMalloc((void **)&d_ki, ki.size() * sizeof(KIRow<R>)));
+        RC_CK(cudaMemcpy(d_ki, ki.data(), ki.size() * sizeof(KIRow<R>), cudaMemcpyHostToDevice));
         c->has_tables = true;
         return RC_OK;
     }
@@ -505,6 +550,8 @@ struct Impl : ImplBase {
             L.yu = d_yu[l];
             L.zu = d_zu[l];
             L.P = s.d_levT[l];
+            L.nbi = (L.im + 3) / 4;
+            L.nbj = (L.jm + 3) / 4;
             for (int w = 0; w < 6; ++w) L.Pw[w] = s.d_lw[l][w];
         }
         d.imax = p.imax;
@@ -538,10 +585,15 @@ struct Impl : ImplBase {
         d.probg = d_probg;
         d.cdf_f = s.d_cdf_f;
         d.cdf_s = s.d_cdf_s;
+        d.den_f = s.d_den_f;
+        d.ibm = s.d_ibm;
+        d.guide_f = s.d_guide_f;
+        d.guide_s = s.d_guide_s;
         d.probq = d_probq;
         d.Ibw = d_Ibw;
         d.Pw0[0] = s.d_Tw0[0];
         d.Pw0[1] = s.d_Tw0[1];
+        d.ki = p.grey ? s.d_ki_grey : d_ki;
         d.sc = s.d_sc;
         d.partial = s.d_partial;
         const long long ncf = (long long)p.imax * p.jmax * c->kloc;
@@ -550,6 +602,27 @@ struct Impl : ImplBase {
         d.n_tiles = (d.n_items + kWarp - 1) / kWarp;
         d.key0 = (uint32_t)p.seed;
         d.key1 = (uint32_t)(p.seed >> 32);
+        d.nwc = (unsigned long long)p.jmax * c->kloc;
+        d.mg_nchunk = magic(d.nchunk);
+        d.mg_nvar = magic(p.nVar);
+        d.mg_imax = magic(p.imax);
+        d.mg_jmax = magic(p.jmax);
+        d.mg_nwc = magic(d.nwc);
+    }
+
+    // Multiply-high reciprocal of a divisor d (see fdiv): floor((2^64-1)/d)+1,
+    // 0 for d = 1.
+    static unsigned long long magic(unsigned long long d) {
+        return d <= 1 ? 0ull : (~0ull / d) + 1ull;
+    }
+
+    // fdiv is exact when numerator * divisor < 2^64 at every division of the
+    // item decomposition.
+    bool decomposition_fits(const DSolve<R> &d) const {
+        const long double lim = 18446744073709551615.0L;
+        const long double n = (long double)d.n_items;
+        return n * d.nchunk < lim && n * d.nVar < lim && n * c->p.imax < lim && n * c->p.jmax < lim &&
+               n * (long double)d.nwc < lim;
     }
 
     size_t partial_count(int rpt) const {
@@ -592,9 +665,11 @@ struct Impl : ImplBase {
             k_grey_ib<R><<<std::max(1, std::min((n + 255) / 256, c->num_sms * 4)), 256, 0, st>>>(s.d_Ibt_grey, Tnb,
                                                                                                   d_wvc, nT, nB);
             Ibt = s.d_Ibt_grey;
+            k_build_ki<R><<<std::max(1, std::min((n + 255) / 256, c->num_sms * 4)), 256, 0, st>>>(s.d_ki_grey, d_kt,
+                                                                                                Ibt, nB, 1, nT);
         }
-        k_setup2<R><<<1, 64, 0, st>>>(s.d_sc, s.d_cdf_f, s.d_cdf_s, d_prob, Ibt, d_wvl, d_wvr, nT, nB, p.grey,
-                                      p.calcwalls);
+        k_setup2<R><<<1, 256, 0, st>>>(s.d_sc, s.d_cdf_f, s.d_cdf_s, s.d_guide_f, s.d_guide_s, s.d_den_f, s.d_ibm,
+                                       d_prob, Ibt, d_kt, d_wvl, d_wvr, nT, nB, nQ, p.grey, p.calcwalls);
         const LevelJobs &J = s.jobs;
         int gl = (int)std::min<long long>((J.total + 255) / 256, (long long)c->num_sms * 8);
         k_levels<R><<<std::max(gl, 1), 256, 0, st>>>(s.d_T, p.imax, p.jmax, p.kmax, J, s.d_sc, nT);
@@ -679,7 +754,11 @@ struct Impl : ImplBase {
         rc = enqueue_setup(s, st);
         if (rc) return rc;
         fill_desc(s, zstart, rpt, *s.h_desc);
+        if (!decomposition_fits(*s.h_desc))
+            return set_err(err_, RC_E_INVALID, "too many work items for one solve: raise rays_per_thread");
         RC_CK(cudaMemcpyAsync(s.d_desc, s.h_desc, sizeof(DSolve<R>), cudaMemcpyHostToDevice, st));
+        k_patch_desc<R><<<1, 32, 0, st>>>(s.d_desc, s.d_sc);
+        RC_CK(cudaGetLastError());
         TallyOut *o = s.h_out;
         o->q64 = s.d_q64;
         o->var64 = s.d_var64;
@@ -1069,7 +1148,12 @@ int rc_create(const rc_params *p, int device, rc_ctx **out) {
     c->grid.resize(p->grid_num);
     for (int l = 0; l < p->grid_num; ++l) build_grid_level(*p, l, c->grid[l]);
     c->dbl = p->floatpoint == 1;
-    c->minb = c->dbl ? 2 : 3;  // FP64 ray state needs the larger register budget
+    // measured best on B200 for the 64^3 narrow-band and 32^3 grey channels:
+    // 4 bundles per work item, 256-thread blocks, 64-register budget (FP32);
+    // the FP64 ray state needs the larger register budget
+    c->rpt = 4;
+    c->block = 256;
+    c->minb = c->dbl ? 2 : 4;
     int rc;
     if (c->dbl) {
         auto *im = new Impl<double>();
@@ -1258,7 +1342,12 @@ int batch_enqueue(rc_batch *b) {
         if (i == 0) block = c->block;
         max_cells = std::max(max_cells, im.tally_cells());
     }
-    RC_CK(cudaMemcpyAsync(b->d_solves, hs, n * sizeof(DSolve<R>), cudaMemcpyHostToDevice, b->st));
+    // descriptors with their run-time fields already patched on the device
+    for (size_t i = 0; i < n; ++i) {
+        Slot<R> &s = *static_cast<Slot<R> *>(b->m[i].slot);
+        RC_CK(cudaMemcpyAsync(static_cast<DSolve<R> *>(b->d_solves) + i, s.d_desc, sizeof(DSolve<R>),
+                              cudaMemcpyDeviceToDevice, b->st));
+    }
     RC_CK(cudaMemcpyAsync(b->d_tiles, b->h_tiles, (n + 1) * sizeof(long long), cudaMemcpyHostToDevice, b->st));
     RC_CK(cudaMemcpyAsync(b->d_outs, b->h_outs, n * sizeof(TallyOut), cudaMemcpyHostToDevice, b->st));
     Impl<R> &im0 = *static_cast<Impl<R> *>(b->m[0].ctx->impl);
