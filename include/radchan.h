@@ -203,6 +203,25 @@ int rc_get_launch(rc_ctx *ctx, int *rays_per_thread, int *block_threads, int *so
  * (pilot_photmax) and keep the fastest; writes the chosen knobs. */
 int rc_autotune(rc_ctx *ctx, const float *T, int zstart, int pilot_photmax,
                 int *rays_per_thread, int *block_threads, int *occupancy);
+/* Solve without allocating device memory (this entry point has no
+ * counterpart in the reference).  For callers that cannot call cudaMalloc
+ * while they run -- a time-stepping code whose device memory is owned by
+ * another allocator or reserved up front, or that must not add allocation
+ * latency or failure points to a step -- this runs the same kernels as
+ * rc_solve_device_async, but the march's partial sums go to a
+ * library-owned static device array of 64 MiB (8,388,608 doubles: one per
+ * cell x replicate x part of the photmax/rays_per_thread decomposition,
+ * plus the wall cells) instead of a buffer the library would allocate.
+ * Sizes beyond that return RC_E_INVALID.  T_dev is the whole field in
+ * device memory; q64/var64 (required) and qw64/vw64 (optional) are the
+ * caller's device arrays in the compact layouts of rc_collect.  The call
+ * returns when the results are written.  The array is set up on the first
+ * call on each device (make that first call before any stream capture) and
+ * keeps its contents between calls; every element a solve reads is written
+ * by the same solve first.  All calls in the process share the one array,
+ * so calls that overlap on the GPU (several contexts or threads) race. */
+int rc_solve_noalloc(rc_ctx *ctx, const float *T_dev, int zstart, double *q64_dev, double *var64_dev,
+                     double *qw64_dev, double *vw64_dev);
 int rc_destroy(rc_ctx *ctx);
 int rc_last_error(const rc_ctx *ctx, char *buf, size_t len);
 /* Grid faces/centres of level `level` as built by the library

@@ -112,6 +112,7 @@ _SIGS = [
     ("rc_set_launch", _I, [_VP, _I, _I, _I, _I]),
     ("rc_get_launch", _I, [_VP, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int)]),
     ("rc_autotune", _I, [_VP, _FP, _I, _I, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+    ("rc_solve_noalloc", _I, [_VP, _VP, _I, _VP, _VP, _VP, _VP]),
     ("rc_destroy", _I, [_VP]),
     ("rc_last_error", _I, [_VP, C.c_char_p, C.c_size_t]),
     ("rc_grid_level", _I, [C.POINTER(RcParams), _I, _FP, _FP, _FP, _FP, _FP, _FP]),

@@ -16,6 +16,7 @@
 #include <algorithm>
 #include <chrono>
 #include <memory>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -1541,3 +1542,105 @@ int rc_batch_destroy(rc_batch *b) {
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Solve into caller-provided device arrays with library-owned scratch, for
+// callers that must not allocate device memory while they run.
+// ---------------------------------------------------------------------------
+namespace {
+
+// Partial sums of the march (one double per (cell, replicate, part)) live in
+// this file-scope device array instead of a cudaMalloc'd buffer.  Every GPU
+// that loads the library holds it until the process exits.
+constexpr size_t kNoAllocScratchBytes = (size_t)64 << 20;  // 64 MiB
+constexpr size_t kNoAllocScratchDoubles = kNoAllocScratchBytes / sizeof(double);
+static __device__ __align__(256) double g_noalloc_scratch[kNoAllocScratchDoubles];
+
+std::mutex g_noalloc_mu;
+double *g_noalloc_ptr[128] = {};
+
+// Device address of the scratch array on `device` (which must be current).
+// In host code g_noalloc_scratch is only a host-side stand-in for the symbol,
+// so the address is looked up once per device and cached.
+int noalloc_scratch(int device, double **out, std::string *err_) {
+    std::lock_guard<std::mutex> lk(g_noalloc_mu);
+    if (device < 0 || device >= 128) return set_err(err_, RC_E_INVALID, "device index out of range");
+    if (!g_noalloc_ptr[device]) {
+        double *p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress((void **)&p, g_noalloc_scratch);
+        if (e != cudaSuccess)
+            return set_err(err_, RC_E_CUDA, std::string("cudaGetSymbolAddress(scratch): ") + cudaGetErrorString(e));
+        g_noalloc_ptr[device] = p;
+    }
+    *out = g_noalloc_ptr[device];
+    return RC_OK;
+}
+
+template <typename R>
+int solve_noalloc_t(rc_ctx *c, const float *T_dev, int zstart, double *q64, double *var64, double *qw64,
+                    double *vw64) {
+    Impl<R> &im = *static_cast<Impl<R> *>(c->impl);
+    std::string *err_ = &c->err;
+    const rc_params &p = c->p;
+    int rc = im.check_solve_args(T_dev, zstart);
+    if (rc) return rc;
+    if (!q64 || !var64) return set_err(err_, RC_E_INVALID, "q64 and var64 output arrays are required");
+    const int rpt = c->rpt;
+    const size_t need = im.partial_count(rpt);
+    if (need > kNoAllocScratchDoubles)
+        return set_err(err_, RC_E_INVALID,
+                       "rc_solve_noalloc: this solve needs " + std::to_string(need) +
+                           " doubles of scratch but the static array holds " +
+                           std::to_string(kNoAllocScratchDoubles) +
+                           " (64 MiB); raise rays_per_thread or use rc_solve_device_async");
+    double *scratch = nullptr;
+    rc = noalloc_scratch(c->device, &scratch, err_);
+    if (rc) return rc;
+    Slot<R> *sp = im.free_slot();
+    if (!sp) return set_err(err_, RC_E_BUSY, "all solve slots in use: collect a ticket first");
+    Slot<R> &s = *sp;
+    cudaStream_t st = s.st;
+    const size_t nfield = (size_t)(p.imax + 2) * (p.jmax + 2) * (p.kmax + 2);
+    RC_CK(cudaMemcpyAsync(s.d_T, T_dev, nfield * sizeof(float), cudaMemcpyDeviceToDevice, st));
+    rc = im.enqueue_setup(s, st);
+    if (rc) return rc;
+    im.fill_desc(s, zstart, rpt, *s.h_desc);
+    s.h_desc->partial = scratch;
+    if (!im.decomposition_fits(*s.h_desc))
+        return set_err(err_, RC_E_INVALID, "too many work items for one solve: raise rays_per_thread");
+    RC_CK(cudaMemcpyAsync(s.d_desc, s.h_desc, sizeof(DSolve<R>), cudaMemcpyHostToDevice, st));
+    k_patch_desc<R><<<1, 32, 0, st>>>(s.d_desc, s.d_sc);
+    RC_CK(cudaGetLastError());
+    TallyOut *o = s.h_out;
+    o->q64 = q64;
+    o->var64 = var64;
+    o->qw64 = qw64;
+    o->vw64 = vw64;
+    o->Qc = s.d_Qc;
+    o->Sc = s.d_Sc;
+    o->Wq = s.d_Wq;
+    o->Ws = s.d_Ws;
+    RC_CK(cudaMemcpyAsync(s.d_out, s.h_out, sizeof(TallyOut), cudaMemcpyHostToDevice, st));
+    s.h_tiles[0] = 0;
+    s.h_tiles[1] = s.h_desc->n_tiles;
+    RC_CK(cudaMemcpyAsync(s.d_tiles, s.h_tiles, 2 * sizeof(long long), cudaMemcpyHostToDevice, st));
+    rc = im.launch_march(s.d_desc, s.d_tiles, 1, s.h_desc->n_tiles, s.d_counter, c->block, rpt, st);
+    if (rc) return rc;
+    rc = im.launch_tally(s.d_desc, s.d_out, 1, im.tally_cells(), st);
+    if (rc) return rc;
+    RC_CK(cudaMemcpyAsync(s.h_sc, s.d_sc, sizeof(DScalars), cudaMemcpyDeviceToHost, st));
+    RC_CK(cudaStreamSynchronize(st));
+    if (s.h_sc->status & 2) return set_err(err_, RC_E_RANGE, "temperature field contains non-finite values");
+    return RC_OK;
+}
+
+}  // namespace
+
+extern "C" int rc_solve_noalloc(rc_ctx *c, const float *T_dev, int zstart, double *q64_dev, double *var64_dev,
+                                double *qw64_dev, double *vw64_dev) {
+    if (!c) return set_err(nullptr, RC_E_INVALID, "NULL context");
+    cudaError_t e = cudaSetDevice(c->device);
+    if (e != cudaSuccess) return set_err(&c->err, RC_E_CUDA, cudaGetErrorString(e));
+    if (c->dbl) return solve_noalloc_t<double>(c, T_dev, zstart, q64_dev, var64_dev, qw64_dev, vw64_dev);
+    return solve_noalloc_t<float>(c, T_dev, zstart, q64_dev, var64_dev, qw64_dev, vw64_dev);
+}
