@@ -1,0 +1,154 @@
+"""Build the reference's own CUDA solver (RadChan src/montecarlo) for the B200.
+
+Recipe (nothing from the reference is copied into this repository):
+  1. copy the reference's solver sources from /root/reference into a temporary
+     directory outside the repository;
+  2. apply the minimal patches CUDA 12.9 and this GPU need
+     - the legacy texture reference tex_Ib (removed in CUDA 12) becomes a
+       texture object with the same clamp / linear-filter settings
+       (mc_gpu_noint.cu:26, :787-791, and every tex2D(tex_Ib, ...));
+     - the grey-gas table reader writes probg[nT][nB][nQ], one row past the end
+       of a global array (read_tables.cpp:169-170); the patch writes
+       probg[i][j][g] so no host memory outside the array is overwritten;
+  3. rewrite the #define values of param.h (and the maxi/maxj/maxk initialisers)
+     for the configuration;
+  4. compile with nvcc for sm_100a with the reference's own flags
+     (--use_fast_math -ftz=true -prec-div=false, Makefile:20-24) together with
+     oracle/ref_driver.cu into oracle/_ref/libref_<config>.so.
+
+The library is a checker: tests/golden/make_ref_fixtures.py runs it on a B200
+(one process per solve, because get_results_ calls cudaDeviceReset) and stores
+its per-cell results as statistical parity fixtures.
+"""
+from __future__ import annotations
+
+import os
+import re
+import shutil
+import subprocess
+import sys
+import tempfile
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
+REF = "/root/reference"
+OUT = os.path.join(HERE, "_ref")
+NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
+
+MC_FILES = ["mc_gpu_noint.cu", "memory_copy_noint.cu", "read_tables.cpp", "definitions.h", "device_functions.h",
+            "functions.h", "memory.h"]
+PARAM_FILES = ["param.h", "NarrowBand.h"]
+
+# Grey-gas channel, 32^3: kappa = 1/m, black walls at 955 K / 573 K, periodic
+# y and z, photmax 64, nVar 4, one grid level.
+CONFIGS = {
+    "grey32": dict(defines=dict(num_gpu="1", p_col="1", imax="32", jmax="32", kmax="32", Lx="2.f",
+                                Ly="6.283185307179586f", Lz="3.141592653589793f", fact_mesh="1.5", nVar="4",
+                                photmax="64", chanHeight="1.0", grid_num="1", num_streams="2", blockdim="128",
+                                nblocks="4096", srt="0", grey="1", calcwalls="0", random="0", floatpoint="0",
+                                epsw="1.f", epse="1.f", epss="1.f", epsn="1.f", epsb="1.f", epst="1.f",
+                                Tww="955", Twe="573", Tws="0", Twn="0", Twb="0", Twt="0", adiabw="0", adiabe="0",
+                                toll="1.0e-3", tollS="1.0e-3", bdw="2", bde="2", bds="1", bdn="1", bdb="1", bdt="1"),
+                   levels=["imax"], levels_j=["jmax"], levels_k=["kmax"]),
+}
+
+
+def _patch_mc(src: str) -> str:
+    old_decl = "texture<myfloat, cudaTextureType2D, cudaReadModeElementType> tex_Ib;"
+    assert old_decl in src
+    src = src.replace(old_decl, "__device__ cudaTextureObject_t rc_tex_Ib_obj;")
+    src = src.replace("tex2D(tex_Ib,", "tex2D<myfloat>(rc_tex_Ib_obj,")
+    bind = re.compile(r"tex_Ib\.addressMode\[0\].*?cudaBindTextureToArray\(tex_Ib, cuArrayI\[gpu\], DescIb\);", re.S)
+    assert bind.search(src)
+    src = bind.sub(
+        "{ cudaResourceDesc rd; memset(&rd, 0, sizeof(rd)); rd.resType = cudaResourceTypeArray;\n"
+        "  rd.res.array.array = cuArrayI[gpu];\n"
+        "  cudaTextureDesc td; memset(&td, 0, sizeof(td));\n"
+        "  td.addressMode[0] = cudaAddressModeClamp; td.addressMode[1] = cudaAddressModeClamp;\n"
+        "  td.filterMode = cudaFilterModeLinear; td.readMode = cudaReadModeElementType; td.normalizedCoords = 0;\n"
+        "  cudaTextureObject_t to; cudaCreateTextureObject(&to, &rd, &td, NULL);\n"
+        "  cudaMemcpyToSymbol(rc_tex_Ib_obj, &to, sizeof(to)); }", src)
+    if "#include <string.h>" not in src:
+        src = "#include <string.h>\n" + src
+    return src
+
+
+def _patch_tables(src: str) -> str:
+    old = re.compile(r"probg\[nT\]\[nB\]\[nQ\] = g;(\s*)probg_h\[m\] = probg\[nT\]\[nB\]\[nQ\];")
+    assert old.search(src)
+    return old.sub(r"probg[i][j][g] = g;\1probg_h[m] = probg[i][j][g];", src)
+
+
+def _patch_param(src: str, cfg: dict) -> str:
+    for k, v in cfg["defines"].items():
+        pat = re.compile(r"^(#define\s+%s\s+)(\S+)" % re.escape(k), re.M)
+        assert pat.search(src), k
+        src = pat.sub(lambda m: m.group(1) + v, src, count=1)
+    for name, vals in (("maxi", cfg["levels"]), ("maxj", cfg["levels_j"]), ("maxk", cfg["levels_k"])):
+        pat = re.compile(r"const int %s\[\] = \{[^}]*\};" % name)
+        assert pat.search(src), name
+        src = pat.sub("const int %s[] = {%s};" % (name, ", ".join(vals)), src, count=1)
+    return src
+
+
+def build(name: str, verbose: bool = False) -> str:
+    cfg = CONFIGS[name]
+    os.makedirs(OUT, exist_ok=True)
+    lib = os.path.join(OUT, "libref_%s.so" % name)
+    tmp = tempfile.mkdtemp(prefix="rc_refbuild_")
+    try:
+        mc = os.path.join(tmp, "src", "montecarlo")
+        pa = os.path.join(tmp, "src", "param")
+        os.makedirs(mc)
+        os.makedirs(pa)
+        for f in MC_FILES:
+            shutil.copy(os.path.join(REF, "src", "montecarlo", f), mc)
+        for f in PARAM_FILES:
+            shutil.copy(os.path.join(REF, "src", "param", f), pa)
+        for path, fn in ((os.path.join(mc, "mc_gpu_noint.cu"), _patch_mc),
+                         (os.path.join(mc, "read_tables.cpp"), _patch_tables),
+                         (os.path.join(pa, "param.h"), lambda t: _patch_param(t, cfg))):
+            with open(path) as f:
+                text = f.read()
+            with open(path, "w") as f:
+                f.write(fn(text))
+        flags = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "--use_fast_math", "-ftz=true",
+                 "-prec-div=false", "-Xcompiler", "-fPIC", "-w"]
+        objs = []
+        for f in ("mc_gpu_noint.cu", "memory_copy_noint.cu", "read_tables.cpp"):
+            o = os.path.join(tmp, f + ".o")
+            cmd = [NVCC] + flags + ["-x", "cu" if f.endswith(".cu") else "c++", "-c", os.path.join(mc, f), "-o", o]
+            r = subprocess.run(cmd, capture_output=True, text=True)
+            if r.returncode:
+                raise RuntimeError("reference build failed on %s:\n%s" % (f, r.stderr[-3000:]))
+            objs.append(o)
+        o = os.path.join(tmp, "ref_driver.o")
+        r = subprocess.run([NVCC] + flags + ["-c", os.path.join(HERE, "ref_driver.cu"), "-o", o], capture_output=True,
+                           text=True)
+        if r.returncode:
+            raise RuntimeError(r.stderr[-3000:])
+        objs.append(o)
+        r = subprocess.run([NVCC, "-gencode", "arch=compute_100a,code=sm_100a", "-shared", "-o", lib] + objs +
+                           ["-L/usr/local/cuda/lib64", "-lcurand", "-Xlinker", "-rpath=/usr/local/cuda/lib64"], capture_output=True, text=True)
+        if r.returncode:
+            raise RuntimeError("reference link failed:\n" + r.stderr[-3000:])
+    finally:
+        shutil.rmtree(tmp, ignore_errors=True)
+    if verbose:
+        print(lib)
+    return lib
+
+
+def build_if_present() -> None:
+    """Build every configuration when the reference sources are available."""
+    if not os.path.isdir(os.path.join(REF, "src", "montecarlo")):
+        return
+    for name in CONFIGS:
+        lib = os.path.join(OUT, "libref_%s.so" % name)
+        if not os.path.exists(lib) or os.path.getmtime(lib) < os.path.getmtime(__file__):
+            build(name)
+
+
+if __name__ == "__main__":
+    for n in (sys.argv[1:] or list(CONFIGS)):
+        build(n, verbose=True)

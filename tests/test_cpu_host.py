@@ -1,0 +1,108 @@
+"""Host-side logic: parameter headers, multigrid geometry, spectral tables
+(reference file formats), and the work decomposition -- no GPU needed."""
+import os
+
+import numpy as np
+import pytest
+
+from radchan_b200 import api
+from radchan_b200 import workloads as W
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+GOLD = os.path.join(HERE, "golden")
+REF_PARAM = "/root/reference/src/param"
+
+
+def test_parse_channel_headers():
+    p = api.params_from_headers(os.path.join(GOLD, "param_channel64.h"), os.path.join(GOLD, "narrowband_channel64.h"))
+    assert (p.imax, p.jmax, p.kmax) == (64, 64, 64)
+    assert abs(p.Ly - 6.283185307179586) < 1e-6 and abs(p.Lz - np.pi) < 1e-6
+    assert p.grid_num == 3
+    assert list(p.maxi)[:3] == [64, 32, 16] and list(p.maxk)[:3] == [64, 32, 16]
+    assert list(p.maxs)[:3] == [5, 5, 100000]
+    assert (p.nVar, p.photmax, p.srt, p.grey, p.calcwalls) == (4, 256, 1, 0, 1)
+    assert (p.adiabw, p.adiabe) == (1, 0)
+    assert list(p.Tw)[:2] == [955.0, 573.0]
+    assert list(p.bd) == [2, 2, 1, 1, 1, 1]
+    assert (p.nT, p.nQ, p.nB) == (64, 8, 100)
+    assert api.validate(p) == ""
+
+
+@pytest.mark.skipif(not os.path.isdir(REF_PARAM), reason="reference headers not mounted")
+def test_parse_reference_headers_as_shipped():
+    p = api.params_from_headers(os.path.join(REF_PARAM, "param.h"), os.path.join(REF_PARAM, "NarrowBand.h"))
+    d = api.default_params()
+    for f in ("imax", "jmax", "kmax", "nVar", "photmax", "grid_num", "srt", "grey", "calcwalls", "nT", "nQ", "nB"):
+        assert getattr(p, f) == getattr(d, f), f
+    assert list(p.maxi)[:9] == list(d.maxi)[:9] and list(p.maxs)[:9] == list(d.maxs)[:9]
+    assert list(p.bd) == list(d.bd)
+    assert p.p_col == 48  # multi-node slab count of the production run
+
+
+@pytest.mark.parametrize("dims,levels", [((32, 32, 32), [(32, 32, 32)]),
+                                         ((64, 48, 40), [(64, 48, 40), (32, 24, 20), (16, 12, 10)]),
+                                         ((406, 8, 8), [(406, 8, 8), (14, 4, 4)]),
+                                         ((17, 9, 5), [(17, 9, 5)])])
+def test_grid_levels_equal_oracle_bit_for_bit(dims, levels):
+    from oracle import oracle as O
+    p = W.channel_params(*dims, levels=levels, maxs=[5] * (len(levels) - 1) + [100000], fact_mesh=1.6)
+    for l in range(len(levels)):
+        a = api.grid_level(p, l)
+        b = O.grid_level(p, l)
+        for k in a:
+            np.testing.assert_array_equal(a[k], b[k])
+        xu = a["xu"]
+        assert xu[0] == 0 and abs(xu[-1] - p.Lx) < 1e-6
+        if p.maxi[0] % 2 == 0:
+            assert np.all(np.diff(xu) > 0)
+        else:
+            # the reference's law (definitions.h:108-123) leaves a zero-width
+            # centre cell when imax is odd
+            assert np.all(np.diff(xu) >= 0) and (np.diff(xu) == 0).sum() == 1
+        # parabolic spacing: finest at the walls, symmetric about the centre
+        np.testing.assert_allclose(xu, p.Lx - xu[::-1], atol=1e-5)
+
+
+def test_synthetic_tables_are_consistent():
+    t = W.tables_nb(nB=50, nQ=8, nT=32).arrays()
+    assert np.all(np.diff(t["wvc"]) > 0) and t["wvl"][0] == 500.0 and t["wvr"][-1] == 10000.0
+    np.testing.assert_allclose(t["wq"].sum(), 1.0, rtol=1e-6)
+    assert np.all(np.diff(t["prob"], axis=1) >= 0) and np.all(t["prob"][:, -1] == 1.0)
+    assert np.all(np.diff(t["probg"], axis=2) >= 0) and np.all(t["probg"][:, :, -1] == 1.0)
+    # k increases with g (xi ascending, exp(1.5 xi))
+    assert np.all(np.diff(t["kq"], axis=2) > 0)
+    assert np.all(t["kP"] > 0)
+
+
+def test_reference_table_files_round_trip(tmp_path):
+    ts = W.tables_nb(nB=12, nQ=8, nT=16)
+    ts.write_dir(tmp_path)
+    names = sorted(os.listdir(tmp_path))
+    assert "planck-mean.txt" in names and "prob_new2.txt" in names and "NarrBand11.txt" in names
+    back = api.TableSet.read_dir(tmp_path, 16, 12, 8)
+    a, b = ts.arrays(), back.arrays()
+    for k in ("Tnb", "wvl", "wvr", "wvc"):
+        np.testing.assert_allclose(b[k], a[k], rtol=2e-6)
+    np.testing.assert_allclose(b["kq"], a["kq"], rtol=1e-5)       # %le: 6 significant digits
+    np.testing.assert_allclose(b["prob"], a["prob"], rtol=1e-7)   # %30.20le
+    np.testing.assert_allclose(b["probg"], a["probg"], rtol=1e-7)
+    # prob_new2.txt: "T j cuprob cuprob_new2[nQ]" per line (nbcorrk/write_tables.cpp:40-53)
+    lines = open(os.path.join(tmp_path, "prob_new2.txt")).read().split("\n")
+    assert len(lines[0].split()) == 3 + 8
+
+
+def test_missing_table_file_is_reported(tmp_path):
+    with pytest.raises(Exception) as e:
+        api.TableSet.read_dir(tmp_path, 16, 12, 8)
+    assert "planck-mean" in str(e.value)
+
+
+def test_field_recipe_walls_and_periodicity():
+    p = W.config_nb_64(photmax=4)
+    T = W.channel_field(p)
+    # face averages equal the wall temperatures; y/z ghosts are periodic images
+    np.testing.assert_allclose((T[:, :, 0] + T[:, :, 1]) / 2, 955.0, rtol=1e-6)
+    np.testing.assert_allclose((T[:, :, -1] + T[:, :, -2]) / 2, 573.0, rtol=1e-6)
+    np.testing.assert_array_equal(T[:, 0, :], T[:, -2, :])
+    np.testing.assert_array_equal(T[0], T[-2])
+    assert 500 < T[1:-1, 1:-1, 1:-1].min() and T[1:-1, 1:-1, 1:-1].max() < 1050
