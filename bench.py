@@ -195,7 +195,9 @@ def run_ours(args, ws, rank, local):
         s.set_launch(rays_per_thread=args.rays_per_thread, block_threads=args.block, occupancy=args.occupancy)
     T_dev = torch.from_numpy(T).to(f"cuda:{dev}")
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=f"cuda:{dev}")
-    kernels_per_solve = 7 + (1 if p.grey else 0)
+    # k_init_scalars, k_tmax, k_setup1, k_setup2, k_levels, k_patch_desc,
+    # k_march, k_tally (+ k_grey_ib, k_build_ki for a grey gas)
+    kernels_per_solve = 8 + (2 if p.grey else 0)
     # warm-up
     for _ in range(args.warmup):
         t = s.solve_device_async(T_dev.data_ptr())

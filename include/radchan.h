@@ -274,7 +274,7 @@ typedef struct rc_request {
 typedef struct rc_result_info {
     double t_submit, t_admit, t_done;   /* seconds, server clock */
     int photmax;                        /* bundles per cell used */
-    float rel_std_maxq;                 /* achieved rel. std at argmax |Q| */
+    float rel_std_maxq;                 /* RMS sigma of the cells with |Q| >= 0.9 max|Q|, over max|Q| */
     int status;
 } rc_result_info;
 int rc_server_create(int device, double hbm_budget_bytes, int max_inflight, rc_server **out);

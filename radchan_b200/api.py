@@ -264,3 +264,75 @@ class Batch:
             self.close()
         except Exception:
             pass
+
+
+@dataclass
+class ServedResult:
+    Q: np.ndarray          # Fortran-layout float result (kloc+2, jmax+2, imax+2)
+    sigma: np.ndarray
+    t_submit: float        # seconds on the server's steady clock
+    t_admit: float
+    t_done: float
+    photmax: int           # bundles per cell the solve used
+    rel_std_maxq: float    # sigma / |Q| at the cell of max |Q|
+
+    @property
+    def latency(self) -> float:
+        return self.t_done - self.t_submit
+
+
+class Server:
+    """Continuous-batching solve server on one GPU (rc_server_*).
+
+    submit() copies the request and returns at once; wait() blocks until the
+    request's result is ready.  Requests run concurrently, sharing every
+    march launch; each result equals the same request solved alone."""
+
+    def __init__(self, device=0, hbm_budget_bytes=150e9, max_inflight=8):
+        self.h = C.c_void_p()
+        L.check(L.lib().rc_server_create(device, float(hbm_budget_bytes), max_inflight, C.byref(self.h)))
+        self._params = {}
+        self._tables = []
+
+    def add_tables(self, tables: TableSet) -> int:
+        ts = C.c_int()
+        L.check(L.lib().rc_server_add_tables(self.h, C.byref(tables.view), C.byref(ts)))
+        self._tables.append(tables)
+        return ts.value
+
+    def submit(self, params: L.RcParams, T: np.ndarray, table_set: int = -1, zstart: int = 1,
+               tolerance: float = 0.0) -> int:
+        p = copy_params(params)
+        T = np.ascontiguousarray(T, dtype=np.float32)
+        if T.shape != field_shape(p):
+            raise ValueError("T must have shape %s" % (field_shape(p),))
+        req = L.RcRequest(C.pointer(p), table_set, T.ctypes.data_as(C.POINTER(C.c_float)), zstart, tolerance)
+        rid = C.c_int64()
+        L.check(L.lib().rc_server_submit(self.h, C.byref(req), C.byref(rid)))
+        self._params[rid.value] = p
+        return rid.value
+
+    def wait(self, rid: int) -> ServedResult:
+        p = self._params.pop(rid)
+        Q = np.zeros(result_shape(p), np.float32)
+        S = np.zeros(result_shape(p), np.float32)
+        info = L.RcResultInfo()
+        fp = lambda a: a.ctypes.data_as(C.POINTER(C.c_float))
+        L.check(L.lib().rc_server_wait(self.h, rid, fp(Q), fp(S), C.byref(info)))
+        return ServedResult(Q, S, info.t_submit, info.t_admit, info.t_done, info.photmax, info.rel_std_maxq)
+
+    def stats(self):
+        a, b, c = C.c_double(), C.c_double(), C.c_double()
+        L.check(L.lib().rc_server_stats(self.h, C.byref(a), C.byref(b), C.byref(c)))
+        return {"solves": a.value, "busy_s": b.value, "hbm_in_use": c.value}
+
+    def close(self):
+        if self.h:
+            L.lib().rc_server_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -108,6 +108,7 @@ struct DSolve {
     unsigned long long mg_nchunk, mg_nvar, mg_imax, mg_jmax, mg_nwc;
     unsigned long long nwc;   // jmax * kloc
     uint32_t key0, key1;
+    long long tile_base;      // first tile of this launch within the solve (server quanta)
 };
 
 // ---------------------------------------------------------------------------

@@ -13,7 +13,7 @@ namespace rc {
 
 // Max of interior T and of the x-wall face averages (mc_gpu_noint.cu:696-710),
 // min of interior T, and finiteness flags.
-__global__ void k_tmax(const float *__restrict__ T, int imax, int jmax, int kmax, DScalars *sc) {
+static __global__ void k_tmax(const float *__restrict__ T, int imax, int jmax, int kmax, DScalars *sc) {
     const long long n = (long long)imax * jmax * kmax;
     float mx = 0.f, mn = 3.4e38f;
     int st = 0;
@@ -113,7 +113,7 @@ __global__ void k_patch_desc(DSolve<R> *d, const DScalars *sc) {
     }
 }
 
-__global__ void k_init_scalars(DScalars *sc) {
+static __global__ void k_init_scalars(DScalars *sc) {
     if (threadIdx.x == 0 && blockIdx.x == 0) {
         DScalars z;
         memset(&z, 0, sizeof(z));

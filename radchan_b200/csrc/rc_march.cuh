@@ -125,7 +125,8 @@ __global__ void __launch_bounds__(256, MINB) k_march(MarchArgs a) {
                             Sp = solves + so;
                             cur_solve = so;
                         }
-                        const long long i0 = (long long)(tile - (unsigned long long)a.tile_start[so]) * kWarp;
+                        const long long i0 =
+                            ((long long)(tile - (unsigned long long)a.tile_start[so]) + Sp->tile_base) * kWarp;
                         if (fpar) item0_1 = i0;
                         else item0_0 = i0;
                         double *sl = slots0 + fpar * pool_max;

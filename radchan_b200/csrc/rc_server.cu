@@ -1,15 +1,660 @@
-// rc_server.cu -- continuous-batching solve server (placeholder until the
-// scheduler lands; every entry point reports RC_E_STATE).
-#include "radchan.h"
+// rc_server.cu -- continuous-batching solve server.
+//
+// The reference solves one field per mc_gpu_ call, synchronously
+// (src/montecarlo/mc_gpu_noint.cu:659-1013).  The server accepts many
+// independent solve requests (temperature field, parameter set, table set,
+// photmax or a target relative standard deviation of max|Q|) and keeps one
+// GPU busy with all of them at once:
+//
+//   * admission in arrival order, bounded by max_inflight and a device-memory
+//     budget; every admitted request takes a pooled solver context whose
+//     grid, tables and buffers stay resident between requests of the same
+//     problem class (everything but photmax and the seed equal);
+//   * one scheduler thread drives the GPU in quanta: a quantum is one
+//     persistent march launch whose work queue holds an equal share of the
+//     remaining tiles of every running request (processor sharing), so a
+//     request that arrives while long solves run joins the next quantum
+//     instead of queueing behind them;
+//   * the request whose last tiles ran in a quantum gets its tally and the
+//     scalar copy-back right after it on the same stream; two quanta are in
+//     flight at a time, so the host builds the next while the GPU runs one.
+//
+// Results are bit-identical to the same request solved alone by a context:
+// every bundle's history depends only on (seed, cell, replicate, bundle),
+// a tile of 32 work items is always marched inside one launch, and partial
+// sums are combined in a fixed order by the tally.
+//
+// A request with a tolerance first runs a pilot solve of 64 bundles per cell
+// (skipped once a request of the same problem class has calibrated the
+// bundle count), then the solve with photmax = n0 (s0 / tol)^2, as the
+// relative Monte Carlo standard deviation falls as photmax^-1/2.
+#include <condition_variable>
+#include <deque>
+#include <map>
+#include <thread>
+
+#include "rc_impl.cuh"
+
+using namespace rc_detail;
+
+namespace rc_detail {
+
+inline double now_s() {
+    return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
+enum SrvStage : int { ST_QUEUED = 0, ST_PILOT = 1, ST_MAIN = 2, ST_DONE = 3, ST_FAILED = 4 };
+enum SrvPhase : int { PH_PREPARE = 0, PH_MARCH = 1, PH_TALLY = 2 };
+
+struct SrvReq {
+    int64_t id = 0;
+    rc_params p;
+    int table_set = -1;
+    std::vector<float> T;
+    int zstart = 1;
+    float tol = 0.f;
+    int stage = ST_QUEUED;
+    int phase = PH_PREPARE;
+    bool published = false;  // result visible to rc_server_wait (guarded by the server mutex)
+    double t_submit = 0, t_admit = 0, t_done = 0;
+    rc_ctx *ctx = nullptr;
+    Slot<float> *slot = nullptr;
+    std::string key;
+    long long tiles = 0, next_tile = 0;
+    int photmax = 0;
+    float rel_std = 0.f;
+    int status = RC_OK;
+    std::string err;
+    cudaEvent_t ev = nullptr;
+    std::vector<float> Q, S;
+};
+
+struct PoolCtx {
+    rc_ctx *ctx;
+    size_t bytes;
+    std::string key;
+    bool busy;
+};
+
+constexpr long long kQuantumTiles = 131072;  // 16.8M bundles at 4 rays per thread
+constexpr long long kMinShare = 4096;
+constexpr int kPilotPhotmax = 64;
+constexpr int kMaxPhotmax = 1 << 20;
+
+}  // namespace rc_detail
+
+struct rc_server {
+    int device = 0;
+    double budget = 0;
+    int max_inflight = 8;
+    std::vector<TableSet> tables;
+    std::mutex mu;
+    std::condition_variable cv_work, cv_done;
+    std::deque<SrvReq *> queue;
+    std::map<int64_t, std::unique_ptr<SrvReq>> reqs;
+    std::vector<SrvReq *> running;
+    std::vector<PoolCtx> pool;
+    std::map<std::string, std::pair<int, float>> calib;  // class -> (photmax, rel std)
+    int64_t next_id = 1;
+    double hbm_in_use = 0;
+    double solves_done = 0, busy_s = 0;
+    bool stop = false;
+    std::thread worker;
+    cudaStream_t st = nullptr;
+    // quantum launch buffers, one set per parity (two quanta in flight)
+    int cap = 0;
+    DSolve<float> *d_solves[2] = {nullptr, nullptr};
+    long long *d_tiles[2] = {nullptr, nullptr};
+    long long *d_base[2] = {nullptr, nullptr};
+    long long *h_tiles[2] = {nullptr, nullptr};
+    long long *h_base[2] = {nullptr, nullptr};
+    unsigned long long *d_counter[2] = {nullptr, nullptr};
+    cudaEvent_t q_start[2] = {nullptr, nullptr}, q_end[2] = {nullptr, nullptr};
+    bool q_used[2] = {false, false};
+    int q_par = 0;
+    std::string err;
+};
+
+namespace rc_detail {
+
+__global__ void k_set_tile_base(DSolve<float> *d, const long long *base, int n) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) d[i].tile_base = base[i];
+}
+
+// Problem class: everything that fixes a context's device layout.
+std::string class_key(const rc_params &p, int table_set) {
+    rc_params q = p;
+    q.photmax = 0;
+    q.seed = 0;
+    std::string k((const char *)&q, sizeof(q));
+    k += "/" + std::to_string(table_set);
+    return k;
+}
+
+// Device bytes of one context (two slots, default 4 rays per thread):
+// the allocations of Impl::init, the tables and the partial-sum array.
+size_t context_bytes(const rc_params &p, int photmax) {
+    const int kl = p.kmax / p.p_col;
+    const double nfield = (double)(p.imax + 2) * (p.jmax + 2) * (p.kmax + 2);
+    const double ncf = (double)p.imax * p.jmax * kl, nwc = 2.0 * p.jmax * kl;
+    double slot = nfield * 4 + ncf * 24 + nwc * 24 + 2.0 * p.jmax * p.kmax * 2;
+    for (int l = 0; l < p.grid_num; ++l) {
+        const double nbr = (double)((p.maxi[l] + 3) / 4) * ((p.maxj[l] + 3) / 4) * ((p.maxk[l] + 3) / 4);
+        slot += nbr * 64 * 2 + 2.0 * ((double)p.maxj[l] * p.maxk[l] + (double)p.maxi[l] * p.maxk[l] +
+                                      (double)p.maxi[l] * p.maxj[l]) * 2;
+    }
+    const int nB = p.grey ? p.grey_nB : p.nB, nT = p.grey ? p.grey_nT : p.nT, nQ = p.grey ? 1 : p.nQ;
+    const double tabs = (double)nB * nQ * nT * (4 + 4 + sizeof(KIRow<float>)) + (double)nB * nT * 8;
+    if (p.grey) slot += (double)nT * nB * (4 + sizeof(KIRow<float>));
+    const int rpt = 4;
+    const long long nchunk = ((long long)std::max(photmax, 1) + rpt - 1) / rpt;
+    const long long nparts = nchunk <= 32 ? 1 : (nchunk + 31) / 32;
+    const double partial = (ncf + nwc) * p.nVar * (double)nparts * 8;
+    return (size_t)(2 * slot + tabs + partial + (1 << 20));
+}
+
+// Relative standard deviation of max|Q|: the RMS sigma of the cells whose
+// |Q| is within 10% of the maximum, over max|Q|.  Pooling those cells keeps
+// the estimate stable when nVar (the replicates behind each sigma) is small.
+float rel_std_maxq(const float *Qc, const float *Sc, size_t n) {
+    float best = 0.f;
+    for (size_t c = 0; c < n; ++c) best = std::max(best, fabsf(Qc[c]));
+    if (!(best > 0.f)) return 0.f;
+    double s2 = 0.0;
+    long long m = 0;
+    for (size_t c = 0; c < n; ++c)
+        if (fabsf(Qc[c]) >= 0.9f * best) {
+            s2 += (double)Sc[c] * Sc[c];
+            ++m;
+        }
+    return (float)(std::sqrt(s2 / (double)m) / best);
+}
+
+int photmax_for(int n0, float s0, float tol) {
+    const double want = (double)n0 * ((double)s0 / tol) * ((double)s0 / tol);
+    return (int)std::min((double)kMaxPhotmax, std::max((double)kPilotPhotmax, std::ceil(want)));
+}
+
+}  // namespace rc_detail
+
+namespace {
+
+// ---- scheduler (worker thread)
+
+int grow_quantum_buffers(rc_server *sv, int n) {
+    std::string *err_ = &sv->err;
+    if (n <= sv->cap) return RC_OK;
+    RC_CK(cudaStreamSynchronize(sv->st));
+    for (int i = 0; i < 2; ++i) {
+        if (sv->d_solves[i]) cudaFree(sv->d_solves[i]);
+        if (sv->d_tiles[i]) cudaFree(sv->d_tiles[i]);
+        if (sv->d_base[i]) cudaFree(sv->d_base[i]);
+        if (sv->h_tiles[i]) cudaFreeHost(sv->h_tiles[i]);
+        if (sv->h_base[i]) cudaFreeHost(sv->h_base[i]);
+        sv->d_solves[i] = nullptr;
+        sv->d_tiles[i] = sv->d_base[i] = sv->h_tiles[i] = sv->h_base[i] = nullptr;
+    }
+    sv->cap = 0;
+    const int c = std::max(n, 64);
+    for (int i = 0; i < 2; ++i) {
+        RC_CK(cudaMalloc((void **)&sv->d_solves[i], c * sizeof(DSolve<float>)));
+        RC_CK(cudaMalloc((void **)&sv->d_tiles[i], (c + 1) * sizeof(long long)));
+        RC_CK(cudaMalloc((void **)&sv->d_base[i], c * sizeof(long long)));
+        RC_CK(cudaHostAlloc((void **)&sv->h_tiles[i], (c + 1) * sizeof(long long), cudaHostAllocDefault));
+        RC_CK(cudaHostAlloc((void **)&sv->h_base[i], c * sizeof(long long), cudaHostAllocDefault));
+    }
+    sv->cap = c;
+    return RC_OK;
+}
+
+size_t idle_bytes(const rc_server *sv) {
+    size_t b = 0;
+    for (const auto &pc : sv->pool)
+        if (!pc.busy) b += pc.bytes;
+    return b;
+}
+
+bool has_idle_context(const rc_server *sv, const std::string &key) {
+    for (const auto &pc : sv->pool)
+        if (!pc.busy && pc.key == key) return true;
+    return false;
+}
+
+// Take a pooled context of the request's class, or create one (evicting
+// idle contexts of other classes while over the budget).
+int acquire_context(rc_server *sv, SrvReq *r) {
+    for (auto &pc : sv->pool)
+        if (!pc.busy && pc.key == r->key) {
+            pc.busy = true;
+            r->ctx = pc.ctx;
+            return RC_OK;
+        }
+    const size_t need = context_bytes(r->p, std::max(r->photmax, kPilotPhotmax));
+    for (size_t i = 0; i < sv->pool.size() && sv->hbm_in_use + need > sv->budget;) {
+        if (!sv->pool[i].busy) {
+            sv->hbm_in_use -= sv->pool[i].bytes;
+            rc_destroy(sv->pool[i].ctx);
+            sv->pool.erase(sv->pool.begin() + i);
+        } else {
+            ++i;
+        }
+    }
+    if (sv->hbm_in_use + need > sv->budget) return set_err(nullptr, RC_E_NOMEM, "HBM budget exhausted");
+    rc_ctx *c = nullptr;
+    int rc = rc_create(&r->p, sv->device, &c);
+    if (rc) return rc;
+    if (!r->p.grey) {
+        rc_tables v;
+        sv->tables[r->table_set].view(&v);
+        rc = rc_set_tables(c, &v);
+        if (rc) {
+            const std::string m = c->err;
+            rc_destroy(c);
+            return set_err(nullptr, rc, m);
+        }
+    }
+    sv->pool.push_back(PoolCtx{c, need, r->key, true});
+    sv->hbm_in_use += need;
+    r->ctx = c;
+    return RC_OK;
+}
+
+void release_context(rc_server *sv, SrvReq *r) {
+    for (auto &pc : sv->pool)
+        if (pc.ctx == r->ctx) pc.busy = false;
+    r->ctx = nullptr;
+}
+
+void fail(rc_server *sv, SrvReq *r, int code, const std::string &m) {
+    r->status = code;
+    r->err = m;
+    r->stage = ST_FAILED;
+    r->t_done = now_s();
+    if (r->slot) r->slot->state = 0;
+    r->slot = nullptr;
+    if (r->ctx) release_context(sv, r);
+}
+
+// Budget share of a context whose partial-sum array grows with photmax.
+void account_photmax(rc_server *sv, SrvReq *r) {
+    for (auto &pc : sv->pool)
+        if (pc.ctx == r->ctx) {
+            const size_t b = context_bytes(r->p, r->photmax);
+            if (b > pc.bytes) {
+                sv->hbm_in_use += (double)(b - pc.bytes);
+                pc.bytes = b;
+            }
+        }
+}
+
+// Field copy, set-up kernels and descriptor of the request's current stage.
+int start_stage(rc_server *sv, SrvReq *r) {
+    Impl<float> &im = *static_cast<Impl<float> *>(r->ctx->impl);
+    r->ctx->p.photmax = r->photmax;
+    r->ctx->p.seed = r->p.seed;
+    account_photmax(sv, r);
+    int rc = im.prepare(*r->slot, nullptr, r->zstart, r->ctx->rpt, sv->st);
+    if (rc) return rc;
+    r->tiles = r->slot->h_desc->n_tiles;
+    r->next_tile = 0;
+    r->phase = PH_MARCH;
+    return RC_OK;
+}
+
+// One quantum: a march launch over equal shares of every marching request's
+// remaining tiles, then the tallies of the requests it completes.
+int run_quantum(rc_server *sv, const std::vector<SrvReq *> &marching, int par) {
+    std::string *err_ = &sv->err;
+    const int n = (int)marching.size();
+    int rc = grow_quantum_buffers(sv, n);
+    if (rc) return rc;
+    long long *ht = sv->h_tiles[par], *hb = sv->h_base[par];
+    ht[0] = 0;
+    const long long share = std::max<long long>(kQuantumTiles / n, kMinShare);
+    int rpt_max = 1;
+    for (int i = 0; i < n; ++i) {
+        SrvReq *r = marching[i];
+        const long long take = std::min(share, r->tiles - r->next_tile);
+        hb[i] = r->next_tile;
+        ht[i + 1] = ht[i] + take;
+        r->next_tile += take;
+        rpt_max = std::max(rpt_max, r->ctx->rpt);
+        RC_CK(cudaMemcpyAsync(sv->d_solves[par] + i, r->slot->d_desc, sizeof(DSolve<float>),
+                              cudaMemcpyDeviceToDevice, sv->st));
+    }
+    RC_CK(cudaMemcpyAsync(sv->d_tiles[par], ht, (n + 1) * sizeof(long long), cudaMemcpyHostToDevice, sv->st));
+    RC_CK(cudaMemcpyAsync(sv->d_base[par], hb, n * sizeof(long long), cudaMemcpyHostToDevice, sv->st));
+    k_set_tile_base<<<(n + 127) / 128, 128, 0, sv->st>>>(sv->d_solves[par], sv->d_base[par], n);
+    RC_CK(cudaGetLastError());
+    if (ht[n] > 0) {
+        Impl<float> &im0 = *static_cast<Impl<float> *>(marching[0]->ctx->impl);
+        rc = im0.launch_march(sv->d_solves[par], sv->d_tiles[par], n, ht[n], sv->d_counter[par],
+                              marching[0]->ctx->block, rpt_max, sv->st);
+        if (rc) return set_err(err_, rc, marching[0]->ctx->err);
+    }
+    for (SrvReq *r : marching) {
+        if (r->next_tile < r->tiles) continue;
+        Impl<float> &im = *static_cast<Impl<float> *>(r->ctx->impl);
+        rc = im.launch_tally(r->slot->d_desc, r->slot->d_out, 1, im.tally_cells(), sv->st);
+        if (rc) return set_err(err_, rc, r->ctx->err);
+        RC_CK(cudaMemcpyAsync(r->slot->h_sc, r->slot->d_sc, sizeof(DScalars), cudaMemcpyDeviceToHost, sv->st));
+        RC_CK(cudaEventRecord(r->ev, sv->st));
+        r->phase = PH_TALLY;
+    }
+    return RC_OK;
+}
+
+// A request whose tally finished: pilot -> main solve, or results -> done.
+void finish_stage(rc_server *sv, SrvReq *r) {
+    Impl<float> &im = *static_cast<Impl<float> *>(r->ctx->impl);
+    Slot<float> &s = *r->slot;
+    const size_t ncf = (size_t)r->p.imax * r->p.jmax * r->ctx->kloc;
+    if (s.h_sc->status & 2) {
+        fail(sv, r, RC_E_RANGE, "temperature field contains non-finite values");
+        return;
+    }
+    if (r->stage == ST_PILOT) {
+        if (cudaMemcpy(s.h_Qc, s.d_Qc, ncf * sizeof(float), cudaMemcpyDeviceToHost) != cudaSuccess ||
+            cudaMemcpy(s.h_Sc, s.d_Sc, ncf * sizeof(float), cudaMemcpyDeviceToHost) != cudaSuccess) {
+            fail(sv, r, RC_E_CUDA, "pilot copy failed");
+            return;
+        }
+        const float s0 = rel_std_maxq(s.h_Qc, s.h_Sc, ncf);
+        r->photmax = s0 > 0 ? photmax_for(r->photmax, s0, r->tol) : kPilotPhotmax;
+        r->stage = ST_MAIN;
+        r->phase = PH_PREPARE;
+        return;
+    }
+    const size_t nres = (size_t)(r->p.imax + 2) * (r->p.jmax + 2) * (r->ctx->kloc + 2);
+    r->Q.assign(nres, 0.f);
+    r->S.assign(nres, 0.f);
+    const int rc = im.copy_out(s, r->Q.data(), r->S.data(), nullptr, nullptr, nullptr, nullptr);
+    if (rc) {
+        fail(sv, r, rc, r->ctx->err);
+        return;
+    }
+    r->rel_std = rel_std_maxq(s.h_Qc, s.h_Sc, ncf);
+    if (r->tol > 0) sv->calib[r->key] = std::make_pair(r->photmax, r->rel_std);
+    s.state = 0;
+    r->slot = nullptr;
+    release_context(sv, r);
+    r->stage = ST_DONE;
+    r->t_done = now_s();
+}
+
+// Admit queued requests in arrival order while they fit.
+void admit(rc_server *sv) {
+    for (;;) {
+        SrvReq *r = nullptr;
+        {
+            std::lock_guard<std::mutex> lk(sv->mu);
+            if (sv->queue.empty() || (int)sv->running.size() >= sv->max_inflight) return;
+            r = sv->queue.front();
+            const size_t need = context_bytes(r->p, std::max(r->photmax, kPilotPhotmax));
+            if (!has_idle_context(sv, r->key) && sv->hbm_in_use - idle_bytes(sv) + need > sv->budget &&
+                !sv->running.empty())
+                return;  // wait for running requests to give memory back
+            sv->queue.pop_front();
+        }
+        r->t_admit = now_s();
+        int rc = acquire_context(sv, r);
+        if (!rc) {
+            Impl<float> &im = *static_cast<Impl<float> *>(r->ctx->impl);
+            r->slot = im.free_slot();
+            r->slot->state = 3;
+            rc = im.stage_host_field(*r->slot, r->T.data());
+            if (rc) g_err = r->ctx->err;
+        }
+        std::lock_guard<std::mutex> lk(sv->mu);
+        if (rc) {
+            fail(sv, r, rc, g_err);
+            r->published = true;
+            sv->cv_done.notify_all();
+            continue;
+        }
+        if (r->tol > 0) {
+            auto it = sv->calib.find(r->key);
+            if (it != sv->calib.end() && it->second.second > 0) {
+                r->photmax = photmax_for(it->second.first, it->second.second, r->tol);
+                r->stage = ST_MAIN;
+            } else {
+                r->photmax = kPilotPhotmax;
+                r->stage = ST_PILOT;
+            }
+        } else {
+            r->stage = ST_MAIN;
+        }
+        r->phase = PH_PREPARE;
+        sv->running.push_back(r);
+    }
+}
+
+void worker_loop(rc_server *sv) {
+    cudaSetDevice(sv->device);
+    for (;;) {
+        {
+            std::lock_guard<std::mutex> lk(sv->mu);
+            if (sv->stop) break;
+        }
+        admit(sv);
+        const int par = sv->q_par;
+        // the quantum issued two iterations ago used this parity's buffers
+        if (sv->q_used[par]) {
+            cudaEventSynchronize(sv->q_end[par]);
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, sv->q_start[par], sv->q_end[par]);
+            sv->busy_s += ms * 1e-3;
+            sv->q_used[par] = false;
+        }
+        // completed tallies
+        bool progressed = false;
+        for (SrvReq *r : sv->running)
+            if (r->phase == PH_TALLY && r->stage < ST_DONE && cudaEventQuery(r->ev) == cudaSuccess) {
+                finish_stage(sv, r);
+                progressed = true;
+            }
+        // set-up of ready stages and one quantum over every marching request
+        std::vector<SrvReq *> marching;
+        bool tallying = false;
+        cudaEventRecord(sv->q_start[par], sv->st);
+        for (SrvReq *r : sv->running) {
+            if (r->stage >= ST_DONE) continue;
+            if (r->phase == PH_PREPARE) {
+                const int rc = start_stage(sv, r);
+                if (rc) {
+                    fail(sv, r, rc, r->ctx ? r->ctx->err : g_err);
+                    continue;
+                }
+            }
+            if (r->phase == PH_MARCH) marching.push_back(r);
+            if (r->phase == PH_TALLY) tallying = true;
+        }
+        if (!marching.empty()) {
+            const int rc = run_quantum(sv, marching, par);
+            if (rc) {
+                cudaStreamSynchronize(sv->st);
+                for (SrvReq *r : marching) fail(sv, r, rc, sv->err);
+            }
+        }
+        cudaEventRecord(sv->q_end[par], sv->st);
+        sv->q_used[par] = true;
+        sv->q_par ^= 1;
+        {
+            std::lock_guard<std::mutex> lk(sv->mu);
+            std::vector<SrvReq *> keep;
+            for (SrvReq *r : sv->running) {
+                if (r->stage >= ST_DONE) {
+                    if (r->stage == ST_DONE) sv->solves_done += 1;
+                    r->published = true;
+                    progressed = true;
+                } else {
+                    keep.push_back(r);
+                }
+            }
+            sv->running.swap(keep);
+            if (progressed) sv->cv_done.notify_all();
+        }
+        if (marching.empty()) {
+            if (tallying) {
+                cudaStreamSynchronize(sv->st);
+            } else {
+                std::unique_lock<std::mutex> lk(sv->mu);
+                if (sv->running.empty())
+                    sv->cv_work.wait_for(lk, std::chrono::milliseconds(5),
+                                         [&] { return sv->stop || !sv->queue.empty(); });
+            }
+        }
+    }
+    cudaStreamSynchronize(sv->st);
+    // requests still queued or running end as failed
+    std::lock_guard<std::mutex> lk(sv->mu);
+    for (SrvReq *r : sv->running) {
+        fail(sv, r, RC_E_STATE, "server destroyed");
+        r->published = true;
+    }
+    sv->running.clear();
+    for (SrvReq *r : sv->queue) {
+        fail(sv, r, RC_E_STATE, "server destroyed");
+        r->published = true;
+    }
+    sv->queue.clear();
+    sv->cv_done.notify_all();
+}
+
+}  // namespace
 
 extern "C" {
-int rc_server_create(int, double, int, rc_server **out) {
-    if (out) *out = nullptr;
-    return RC_E_STATE;
+
+int rc_server_create(int device, double hbm_budget_bytes, int max_inflight, rc_server **out) {
+    if (!out) return set_err(nullptr, RC_E_INVALID, "NULL argument");
+    if (max_inflight < 1) return set_err(nullptr, RC_E_INVALID, "max_inflight must be >= 1");
+    cudaError_t e = cudaSetDevice(device);
+    if (e != cudaSuccess) return set_err(nullptr, RC_E_CUDA, cudaGetErrorString(e));
+    auto *sv = new rc_server();
+    sv->device = device;
+    sv->budget = hbm_budget_bytes > 0 ? hbm_budget_bytes : 150e9;
+    sv->max_inflight = max_inflight;
+    bool ok = cudaStreamCreateWithFlags(&sv->st, cudaStreamNonBlocking) == cudaSuccess;
+    for (int i = 0; i < 2 && ok; ++i)
+        ok = cudaMalloc((void **)&sv->d_counter[i], sizeof(unsigned long long)) == cudaSuccess &&
+             cudaEventCreate(&sv->q_start[i]) == cudaSuccess && cudaEventCreate(&sv->q_end[i]) == cudaSuccess;
+    if (!ok) {
+        rc_server_destroy(sv);
+        return set_err(nullptr, RC_E_CUDA, "server stream/event creation failed");
+    }
+    sv->worker = std::thread(worker_loop, sv);
+    *out = sv;
+    return RC_OK;
 }
-int rc_server_add_tables(rc_server *, const rc_tables *, int *) { return RC_E_STATE; }
-int rc_server_submit(rc_server *, const rc_request *, int64_t *) { return RC_E_STATE; }
-int rc_server_wait(rc_server *, int64_t, float *, float *, rc_result_info *) { return RC_E_STATE; }
-int rc_server_stats(rc_server *, double *, double *, double *) { return RC_E_STATE; }
-int rc_server_destroy(rc_server *) { return RC_OK; }
+
+int rc_server_add_tables(rc_server *sv, const rc_tables *t, int *table_set) {
+    if (!sv || !t || !table_set) return set_err(nullptr, RC_E_INVALID, "NULL argument");
+    TableSet ts;
+    ts.from_view(t);
+    std::lock_guard<std::mutex> lk(sv->mu);
+    sv->tables.push_back(std::move(ts));
+    *table_set = (int)sv->tables.size() - 1;
+    return RC_OK;
 }
+
+int rc_server_submit(rc_server *sv, const rc_request *req, int64_t *id) {
+    if (!sv || !req || !req->params || !req->T || !id) return set_err(nullptr, RC_E_INVALID, "NULL argument");
+    std::string err;
+    if (params_validate(*req->params, err)) return set_err(nullptr, RC_E_INVALID, err);
+    if (req->params->floatpoint) return set_err(nullptr, RC_E_INVALID, "the server runs FP32 march solves only");
+    if (!(req->tolerance >= 0.f)) return set_err(nullptr, RC_E_INVALID, "tolerance must be >= 0");
+    if (req->tolerance == 0.f && req->params->photmax < 1)
+        return set_err(nullptr, RC_E_INVALID, "photmax must be >= 1 when no tolerance is given");
+    const int kl = req->params->kmax / req->params->p_col;
+    const int zs = req->zstart > 0 ? req->zstart : 1;
+    if (zs + kl - 1 > req->params->kmax) return set_err(nullptr, RC_E_INVALID, "zstart out of range");
+    auto r = std::make_unique<SrvReq>();
+    r->p = *req->params;
+    const size_t nf = (size_t)(r->p.imax + 2) * (r->p.jmax + 2) * (r->p.kmax + 2);
+    r->T.assign(req->T, req->T + nf);
+    r->zstart = zs;
+    r->tol = req->tolerance;
+    r->photmax = req->tolerance > 0 ? 0 : req->params->photmax;
+    r->t_submit = now_s();
+    std::lock_guard<std::mutex> lk(sv->mu);
+    if (!r->p.grey && (req->table_set < 0 || req->table_set >= (int)sv->tables.size()))
+        return set_err(nullptr, RC_E_INVALID, "unknown table set");
+    r->table_set = r->p.grey ? -1 : req->table_set;
+    r->key = class_key(r->p, r->table_set);
+    if ((double)context_bytes(r->p, std::max(r->photmax, kPilotPhotmax)) > sv->budget)
+        return set_err(nullptr, RC_E_NOMEM, "request larger than the HBM budget");
+    if (sv->stop) return set_err(nullptr, RC_E_STATE, "server is shutting down");
+    if (cudaEventCreateWithFlags(&r->ev, cudaEventDisableTiming) != cudaSuccess)
+        return set_err(nullptr, RC_E_CUDA, "event creation failed");
+    r->id = sv->next_id++;
+    *id = r->id;
+    sv->queue.push_back(r.get());
+    sv->reqs[r->id] = std::move(r);
+    sv->cv_work.notify_all();
+    return RC_OK;
+}
+
+int rc_server_wait(rc_server *sv, int64_t id, float *Q, float *sigma, rc_result_info *info) {
+    if (!sv) return set_err(nullptr, RC_E_INVALID, "NULL server");
+    std::unique_lock<std::mutex> lk(sv->mu);
+    auto it = sv->reqs.find(id);
+    if (it == sv->reqs.end()) return set_err(nullptr, RC_E_NOTFOUND, "unknown request id");
+    SrvReq *r = it->second.get();
+    sv->cv_done.wait(lk, [&] { return r->published; });
+    if (Q && !r->Q.empty()) memcpy(Q, r->Q.data(), r->Q.size() * sizeof(float));
+    if (sigma && !r->S.empty()) memcpy(sigma, r->S.data(), r->S.size() * sizeof(float));
+    if (info) {
+        info->t_submit = r->t_submit;
+        info->t_admit = r->t_admit;
+        info->t_done = r->t_done;
+        info->photmax = r->photmax;
+        info->rel_std_maxq = r->rel_std;
+        info->status = r->status;
+    }
+    const int st = r->status;
+    const std::string m = r->err;
+    if (r->ev) cudaEventDestroy(r->ev);
+    sv->reqs.erase(it);
+    if (st) return set_err(nullptr, st, m);
+    return RC_OK;
+}
+
+int rc_server_stats(rc_server *sv, double *solves, double *busy_s, double *hbm_in_use) {
+    if (!sv) return set_err(nullptr, RC_E_INVALID, "NULL server");
+    std::lock_guard<std::mutex> lk(sv->mu);
+    if (solves) *solves = sv->solves_done;
+    if (busy_s) *busy_s = sv->busy_s;
+    if (hbm_in_use) *hbm_in_use = sv->hbm_in_use;
+    return RC_OK;
+}
+
+int rc_server_destroy(rc_server *sv) {
+    if (!sv) return RC_OK;
+    {
+        std::lock_guard<std::mutex> lk(sv->mu);
+        sv->stop = true;
+        sv->cv_work.notify_all();
+    }
+    if (sv->worker.joinable()) sv->worker.join();
+    cudaSetDevice(sv->device);
+    if (sv->st) cudaStreamSynchronize(sv->st);
+    for (auto &pc : sv->pool) rc_destroy(pc.ctx);
+    for (auto &kv : sv->reqs)
+        if (kv.second->ev) cudaEventDestroy(kv.second->ev);
+    for (int i = 0; i < 2; ++i) {
+        if (sv->d_solves[i]) cudaFree(sv->d_solves[i]);
+        if (sv->d_tiles[i]) cudaFree(sv->d_tiles[i]);
+        if (sv->d_base[i]) cudaFree(sv->d_base[i]);
+        if (sv->h_tiles[i]) cudaFreeHost(sv->h_tiles[i]);
+        if (sv->h_base[i]) cudaFreeHost(sv->h_base[i]);
+        if (sv->d_counter[i]) cudaFree(sv->d_counter[i]);
+        if (sv->q_start[i]) cudaEventDestroy(sv->q_start[i]);
+        if (sv->q_end[i]) cudaEventDestroy(sv->q_end[i]);
+    }
+    if (sv->st) cudaStreamDestroy(sv->st);
+    delete sv;
+    return RC_OK;
+}
+
+}  // extern "C"

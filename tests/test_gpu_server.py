@@ -1,0 +1,116 @@
+"""Continuous-batching server (rc_server_*): every request solved in a mix
+equals the same request solved alone, bit for bit; tolerance-driven requests
+reach their target; admission respects the device-memory budget."""
+import numpy as np
+import pytest
+
+from radchan_b200 import _lib as L
+from radchan_b200 import api
+from radchan_b200 import workloads as W
+
+pytestmark = [pytest.mark.gpu, pytest.mark.timeout(600)]
+
+
+def _mix():
+    tabs = W.tables_nb(nB=40, nQ=4, nT=32)
+    out = []
+    for s in range(3):
+        p = W.config_grey_32(photmax=64 * (s + 1), nVar=4)
+        p.seed = 1000 + s
+        out.append((p, None, W.channel_field(p, seed=s)))
+    p = W.channel_params(32, 16, 16, photmax=96, nVar=4, nB=40, nQ=4, nT=32,
+                         levels=[(32, 16, 16), (16, 8, 8)], maxs=[5, 100000], calcwalls=1, adiabw=1)
+    out.append((p, tabs, W.channel_field(p, seed=11)))
+    p2 = api.copy_params(p)
+    p2.photmax = 256
+    p2.seed = 77
+    out.append((p2, tabs, W.channel_field(p2, seed=12)))
+    return out
+
+
+def test_mix_equals_alone_bit_for_bit():
+    mix = _mix()
+    alone = []
+    for p, tabs, T in mix:
+        s = api.Solver(p, tabs)
+        r = s.solve(T, want64=False)
+        alone.append((r.Q.copy(), r.sigma.copy()))
+        s.close()
+    srv = api.Server(max_inflight=8)
+    sets = {}
+    ids = []
+    for p, tabs, T in mix:
+        ts = -1
+        if tabs is not None:
+            if id(tabs) not in sets:
+                sets[id(tabs)] = srv.add_tables(tabs)
+            ts = sets[id(tabs)]
+        ids.append(srv.submit(p, T, table_set=ts))
+    for (Qa, Sa), rid, (p, _, _) in zip(alone, ids, mix):
+        r = srv.wait(rid)
+        assert r.photmax == p.photmax
+        np.testing.assert_array_equal(r.Q, Qa)
+        np.testing.assert_array_equal(r.sigma, Sa)
+        assert r.t_submit <= r.t_admit <= r.t_done
+    st = srv.stats()
+    assert st["solves"] == len(mix) and st["busy_s"] > 0
+    # a second round reuses the pooled contexts and gives the same answers
+    ids = [srv.submit(p, T, table_set=(sets[id(t)] if t is not None else -1)) for p, t, T in mix]
+    for (Qa, _), rid in zip(alone, ids):
+        np.testing.assert_array_equal(srv.wait(rid).Q, Qa)
+    srv.close()
+
+
+def test_tolerance_request_reaches_target():
+    p = W.config_grey_32(photmax=1, nVar=4)
+    T = W.channel_field(p, seed=5)
+    srv = api.Server()
+    tol = 0.01
+    r = srv.wait(srv.submit(p, T, tolerance=tol))
+    assert r.photmax > 64
+    assert r.rel_std_maxq < 1.3 * tol
+    # the next request of the same class skips the pilot and uses the calibration
+    r2 = srv.wait(srv.submit(p, W.channel_field(p, seed=6), tolerance=tol))
+    assert abs(r2.photmax - r.photmax) <= 0.3 * r.photmax
+    assert r2.rel_std_maxq < 1.3 * tol
+    srv.close()
+
+
+def test_budget_rejects_oversized_request_and_serialises_admission():
+    p = W.config_grey_32(photmax=64)
+    T = W.channel_field(p)
+    srv = api.Server(hbm_budget_bytes=1e6)
+    with pytest.raises(L.RadChanError) as e:
+        srv.submit(p, T)
+    assert "budget" in str(e.value)
+    srv.close()
+    # the device bytes the server charges for one context of this class
+    srv = api.Server()
+    srv.wait(srv.submit(p, T))
+    one = srv.stats()["hbm_in_use"]
+    srv.close()
+    assert one > 1e6
+    # a budget that holds one context: requests of two classes run one after
+    # the other, the idle context of the first is evicted for the second
+    p2 = api.copy_params(p)
+    p2.abscoeff = 2.0
+    budget = 1.5 * one
+    srv = api.Server(hbm_budget_bytes=budget)
+    a = srv.submit(p, T)
+    b = srv.submit(p2, T)
+    ra, rb = srv.wait(a), srv.wait(b)
+    assert rb.t_admit >= ra.t_done
+    assert srv.stats()["hbm_in_use"] <= budget
+    srv.close()
+
+
+def test_submit_validation():
+    p = W.config_grey_32(photmax=0)
+    T = W.channel_field(W.config_grey_32())
+    srv = api.Server()
+    with pytest.raises(L.RadChanError):
+        srv.submit(p, T)  # neither photmax nor tolerance
+    pn = W.channel_params(16, 8, 8, photmax=16)
+    with pytest.raises(L.RadChanError):
+        srv.submit(pn, W.channel_field(pn), table_set=3)  # unknown table set
+    srv.close()
