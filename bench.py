@@ -13,6 +13,17 @@ kernel), seeded synthetic field and tables.  One step = one full solve.
   roofline  march kernel: ray-cell steps x 32 B (one sector per temperature
          gather) / march time vs the measured HBM copy bandwidth.
 
+Legs on one GPU (skipped with --no-legs):
+  at_1pct  the same solve with photmax raised until the relative std of
+         max|Q| is 1%: solves/s and bundles/s at that tolerance;
+  batched  64 uneven problems (grids 16..96 per axis, half grey, half
+         narrow-band 20-100 bands, photmax 32/128/512): plain one solve per
+         launch vs one persistent launch from a CUDA graph vs the
+         continuous-batching server, solves/s by wall clock.
+
+--serve runs the open-loop serving benchmark instead (Poisson arrivals at
+--load x measured capacity, tolerance-driven photmax, p50/p99 latency).
+
 --impl reference times the CPU restatement of the reference's ray loop
 (the reference has no CPU implementation of this path) on all host cores.
 """
@@ -31,7 +42,7 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-BUNDLE_METRIC = "bundles/s"
+BUNDLE_METRIC = "bundles/s & solves/s at 1% MC std, batched/served vs plain; serve p50/p99"
 
 
 def peaks():
@@ -145,14 +156,14 @@ def cpu_sample(p, tabs, T, seconds=12.0, nthreads=0):
     from oracle import oracle as O
     ncells = p.imax * p.jmax * (p.kmax // p.p_col)
     n = 64
-    t0 = time.perf_counter()
-    r = O.solve(p, tabs, T, rpt=8, cell_begin=0, cell_end=n, walls=False, nthreads=nthreads)
-    dt = time.perf_counter() - t0
-    n2 = int(min(ncells, max(n, n * seconds / max(dt, 1e-3))))
-    t0 = time.perf_counter()
-    r = O.solve(p, tabs, T, rpt=8, cell_begin=0, cell_end=n2, walls=False, nthreads=nthreads)
-    dt = time.perf_counter() - t0
-    return dict(bundles=r["bundles"], steps=r["steps"], seconds=dt, cells=n2)
+    for _ in range(5):
+        t0 = time.perf_counter()
+        r = O.solve(p, tabs, T, rpt=8, cell_begin=0, cell_end=n, walls=False, nthreads=nthreads)
+        dt = time.perf_counter() - t0
+        if dt >= 0.5 * seconds or n >= ncells:
+            break
+        n = int(min(ncells, max(2 * n, n * seconds / max(dt, 1e-3))))
+    return dict(bundles=r["bundles"], steps=r["steps"], seconds=dt, cells=n)
 
 
 def run_reference(args, ws, rank):
@@ -180,6 +191,227 @@ def run_reference(args, ws, rank):
             "steps_per_s": tot_s / tot_t,
             "cpu_baseline": {"value": v, "unit": "bundles/s", "cores": cores, "kind": "port", "sample": sample},
             "e2e": {"value": v, "unit": "bundles/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def leg_at_tolerance(p, tabs, T, rel0, dev, flush, tol=0.01, steps=2):
+    """The same solve with photmax raised until the relative standard
+    deviation of max|Q| is `tol` (it falls as photmax^-1/2): device time per
+    solve, solves/s and bundles/s at that tolerance."""
+    import math
+
+    import torch
+
+    from radchan_b200 import api
+    q = api.copy_params(p)
+    q.photmax = int(math.ceil(p.photmax * (rel0 / tol) ** 2))
+    s = api.Solver(q, tabs, device=dev)
+    T_dev = torch.from_numpy(T).to(f"cuda:{dev}")
+    t = s.solve_device_async(T_dev.data_ptr())
+    s.wait_device(t)
+    s.release(t)
+    ms, bundles, rel = [], 0.0, None
+    for k in range(steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        t = s.solve_device_async(T_dev.data_ptr())
+        info = s.info(t)
+        ms.append(info.ms_solve)
+        bundles += info.bundles
+        if k == steps - 1:
+            r = s.collect(t)
+            rel = api.rel_std_maxq(r.q64, np.sqrt(r.var64))
+        else:
+            s.release(t)
+    s.close()
+    sec = sum(ms) / 1000.0
+    return {"tolerance": tol, "photmax": q.photmax, "rel_std_maxq": rel, "ms_per_solve": 1000 * sec / steps,
+            "solves_per_s": steps / sec, "bundles_per_s": bundles / sec, "steps": steps}
+
+
+def batch_setup(dev, n=64):
+    """The uneven-problem mix: 64 problems, grid edges from
+    {16,24,32,48,64,96} per axis, half grey and half narrow-band (20-100
+    bands x 8 g), photmax from {32,128,512}; seeded fields and tables."""
+    from radchan_b200 import api
+    from radchan_b200 import workloads as W
+    probs = W.batch_problems(n=n)
+    items = []
+    for pr in probs:
+        p = pr["params"]
+        tabs = None if pr["grey"] else W.tables_nb(nB=pr["nB"], nQ=8, nT=64, seed=pr["table_seed"])
+        T = W.channel_field(p, seed=pr["field_seed"])
+        s = api.Solver(p, tabs, device=dev)
+        Q = np.zeros(api.result_shape(p), np.float32)
+        S = np.zeros(api.result_shape(p), np.float32)
+        items.append(dict(p=p, tabs=tabs, T=T, s=s, Q=Q, S=S))
+    return items
+
+
+def leg_batched(dev, passes=2):
+    """Plain (one solve per launch, host arrays in and out, one after the
+    other) vs batched (every solve in one persistent launch replayed from a
+    CUDA graph) vs served (all submitted to the continuous-batching server at
+    once) on the uneven mix.  Wall clock per pass of all 64 solves."""
+    from radchan_b200 import api
+    items = batch_setup(dev)
+    work = [it["p"].imax * it["p"].jmax * it["p"].kmax * it["p"].nVar * it["p"].photmax for it in items]
+    big = items[int(np.argmax(work))]
+    knobs = big["s"].autotune(big["T"], pilot_photmax=min(big["p"].photmax, 128))
+    for it in items:
+        it["s"].set_launch(*knobs)
+    bundles = float(sum(work))
+
+    def plain_pass():
+        t0 = time.perf_counter()
+        for it in items:
+            it["s"].collect_into(it["s"].solve_async(it["T"]), it["Q"], it["S"])
+        return time.perf_counter() - t0
+
+    plain_pass()
+    t_plain = min(plain_pass() for _ in range(passes))
+    ref = [it["Q"].copy() for it in items]
+    b = api.Batch(device=dev, use_graph=True)
+    for it in items:
+        b.add(it["s"], it["T"])
+
+    def batched_pass():
+        t0 = time.perf_counter()
+        b.run()
+        b.wait()
+        for i, it in enumerate(items):
+            b.collect_into(i, it["Q"], it["S"])
+        return time.perf_counter() - t0
+
+    batched_pass()
+    t_batch = min(batched_pass() for _ in range(passes))
+    identical = all(np.array_equal(r, it["Q"]) for r, it in zip(ref, items))
+    b.close()
+    srv = api.Server(device=dev, max_inflight=len(items))
+
+    def served_pass():
+        t0 = time.perf_counter()
+        ids = [srv.submit(it["p"], it["T"], table_set=-1 if it["tabs"] is None else it["ts"]) for it in items]
+        for rid in ids:
+            srv.wait(rid)
+        return time.perf_counter() - t0
+
+    for it in items:
+        if it["tabs"] is not None:
+            it["ts"] = srv.add_tables(it["tabs"])
+    served_pass()
+    t_srv = min(served_pass() for _ in range(passes))
+    srv.close()
+    for it in items:
+        it["s"].close()
+    n = len(items)
+    return {"problems": n, "bundles_per_pass": bundles,
+            "autotuned": {"rays_per_thread": knobs[0], "block_threads": knobs[1], "sort_bands": knobs[2],
+                          "occupancy": knobs[3]},
+            "plain_solves_per_s": n / t_plain, "batched_solves_per_s": n / t_batch, "served_solves_per_s": n / t_srv,
+            "batched_vs_plain": t_plain / t_batch, "served_vs_plain": t_plain / t_srv,
+            "plain_bundles_per_s": bundles / t_plain, "batched_bundles_per_s": bundles / t_batch,
+            "batched_equals_plain": identical, "timing": "wall clock per pass of all solves, host arrays in/out, "
+                                                        "best of %d" % passes}
+
+
+def run_serve(args, rank, local):
+    """Open-loop serving: Poisson arrivals of narrow-band solve requests
+    (100 bands x 8 g) with grids drawn log-uniformly from 32^3 to
+    256x128x128 (eight size classes), tolerance drawn log-uniformly from
+    1% to 5% relative std of max|Q| (photmax chosen by the server), fields
+    and tables resident, admission by a 150 GB budget.  The arrival rate is
+    args.load x the capacity measured with a closed burst of the same mix."""
+    if rank != 0:
+        return
+    import threading
+
+    from radchan_b200 import api
+    from radchan_b200 import workloads as W
+    rng = np.random.default_rng(2024)
+    tabs = W.tables_nb()
+    classes = []
+    for c in range(8):
+        r = c / 7.0
+        im = int(round(32 * 8 ** r / 8)) * 8
+        jm = int(round(32 * 4 ** r / 8)) * 8
+        p = W.channel_params(im, jm, jm, photmax=64, nVar=4, levels=[(im, jm, jm), (im // 2, jm // 2, jm // 2),
+                                                                     (im // 4, jm // 4, jm // 4)],
+                             maxs=[5, 5, 100000], calcwalls=1, adiabw=1)
+        classes.append((p, W.channel_field(p, seed=100 + c)))
+    srv = api.Server(device=local, hbm_budget_bytes=150e9, max_inflight=args.serve_inflight)
+    ts = srv.add_tables(tabs)
+
+    def draw(n):
+        out = []
+        for _ in range(n):
+            c = int(rng.integers(0, 8))
+            tol = float(np.exp(rng.uniform(np.log(0.01), np.log(0.05))))
+            out.append((c, tol))
+        return out
+
+    # calibration of every class (pilot + one solve at 3%), then the service
+    # time of each class alone at its calibrated photmax (no other request)
+    alone = []
+    for p, T in classes:
+        srv.wait(srv.submit(p, T, table_set=ts, tolerance=0.03))
+        r = srv.wait(srv.submit(p, T, table_set=ts, tolerance=0.03))
+        alone.append((r.t_done - r.t_admit, r.photmax))
+    burst = draw(args.serve_burst)
+    t0 = time.perf_counter()
+    ids = [srv.submit(classes[c][0], classes[c][1], table_set=ts, tolerance=tol) for c, tol in burst]
+    for rid in ids:
+        srv.wait(rid)
+    cap = len(burst) / (time.perf_counter() - t0)
+    rate = args.load * cap
+    reqs = draw(args.serve_requests)
+    gaps = rng.exponential(1.0 / rate, size=len(reqs))
+    results = [None] * len(reqs)
+    ids = [None] * len(reqs)
+    ready = threading.Semaphore(0)
+
+    def waiter():
+        for i in range(len(reqs)):
+            ready.acquire()
+            results[i] = srv.wait(ids[i])
+
+    th = threading.Thread(target=waiter)
+    th.start()
+    st0 = srv.stats()
+    t0 = time.perf_counter()
+    t_next = t0
+    for i, (c, tol) in enumerate(reqs):
+        t_next += gaps[i]
+        d = t_next - time.perf_counter()
+        if d > 0:
+            time.sleep(d)
+        ids[i] = srv.submit(classes[c][0], classes[c][1], table_set=ts, tolerance=tol)
+        ready.release()
+    th.join()
+    wall = time.perf_counter() - t0
+    st1 = srv.stats()
+    srv.close()
+    lat = np.array([r.latency for r in results])
+    # service time alone, scaled by photmax from the class's calibration solve
+    svc = np.array([alone[c][0] * r.photmax / alone[c][1] for r, (c, _) in zip(results, reqs)])
+    slow = lat / svc
+    met = np.array([r.rel_std_maxq <= 1.25 * tol for r, (_, tol) in zip(results, reqs)])
+    line = {"metric": "serve latency p50/p99 and solves/s", "impl": "ours", "n_gpus": 1,
+            "requests": len(reqs), "load": args.load, "capacity_solves_per_s": cap,
+            "offered_solves_per_s": rate, "solves_per_s": len(reqs) / wall,
+            "p50_s": float(np.percentile(lat, 50)), "p99_s": float(np.percentile(lat, 99)),
+            "p99_over_p50": float(np.percentile(lat, 99) / np.percentile(lat, 50)),
+            "alone_p50_s": float(np.percentile(svc, 50)), "alone_p99_s": float(np.percentile(svc, 99)),
+            "alone_p99_over_p50": float(np.percentile(svc, 99) / np.percentile(svc, 50)),
+            "slowdown_p50": float(np.percentile(slow, 50)), "slowdown_p99": float(np.percentile(slow, 99)),
+            "mean_photmax": float(np.mean([r.photmax for r in results])),
+            "tolerance_met_frac": float(met.mean()),
+            "gpu_busy_frac": (st1["busy_s"] - st0["busy_s"]) / wall, "hbm_in_use_gb": st1["hbm_in_use"] / 1e9,
+            "data": "synthetic",
+            "config": {"workload": "Poisson stream, narrow-band 100x8, grids 32^3..256x128x128 in 8 log-spaced "
+                                   "classes, tolerance 1-5% log-uniform, 150 GB budget",
+                       "classes": [[p.imax, p.jmax, p.kmax] for p, _ in classes],
+                       "max_inflight": args.serve_inflight, "burst": len(burst)}}
     print(json.dumps(line), flush=True)
 
 
@@ -221,8 +453,7 @@ def run_ours(args, ws, rank, local):
         steps += info.steps
         if k == args.steps - 1:
             r = s.collect(t)
-            i = np.unravel_index(np.argmax(np.abs(r.q64)), r.q64.shape)
-            rel_std = float(np.sqrt(r.var64[i]) / abs(r.q64[i]))
+            rel_std = api.rel_std_maxq(r.q64, np.sqrt(r.var64))
         else:
             s.release(t)
     torch.cuda.synchronize()
@@ -260,6 +491,9 @@ def run_ours(args, ws, rank, local):
             "rel_std_maxq": rel_std, "march_ms": 1000 * march_s / args.steps,
             "roofline": roof, "e2e": e2e, "gpu_launches": kernels_per_solve * args.steps,
             "clocks": clk, "wall_s": wall}
+    if ws == 1 and not args.no_legs:
+        line["at_1pct"] = leg_at_tolerance(p, tabs, T, rel_std, dev, flush)
+        line["batched"] = leg_batched(dev)
     if rank == 0 and not args.no_cpu_baseline:
         cb = cpu_sample(p, tabs, T, seconds=args.ref_seconds)
         line["cpu_baseline"] = {"value": cb["bundles"] / cb["seconds"], "unit": "bundles/s",
@@ -285,9 +519,18 @@ def main():
     ap.add_argument("--traffic", type=float, default=None)
     ap.add_argument("--photmax", type=int, default=0, help="override bundles per cell (profiling runs)")
     ap.add_argument("--no-cpu-baseline", dest="no_cpu_baseline", action="store_true")
+    ap.add_argument("--no-legs", dest="no_legs", action="store_true",
+                    help="skip the 1%%-tolerance and batched-mix legs (profiling runs)")
+    ap.add_argument("--serve", action="store_true", help="open-loop serving run instead of the solve benchmark")
+    ap.add_argument("--serve-requests", dest="serve_requests", type=int, default=200)
+    ap.add_argument("--serve-burst", dest="serve_burst", type=int, default=40)
+    ap.add_argument("--serve-inflight", dest="serve_inflight", type=int, default=8)
+    ap.add_argument("--load", type=float, default=0.8)
     args = ap.parse_args()
     ws, rank, local = dist_init()
-    if args.impl == "reference":
+    if args.serve:
+        run_serve(args, rank, local)
+    elif args.impl == "reference":
         run_reference(args, ws, rank)
     else:
         run_ours(args, ws, rank, local)

@@ -193,16 +193,20 @@ int rc_solve_info_get(rc_ctx *ctx, rc_ticket ticket, rc_solve_info *info);
 /* Launch knobs of the march kernel; values <= 0 (sort_bands < 0) keep the
  * current setting.  rays_per_thread: bundles per work item (power of two
  * <= 64; it fixes the FP64 summation grouping, results differ only by
- * rounding); block_threads: 128 or 256; sort_bands: band-sorted bundle
- * order within a warp's pool (srt); occupancy: resident 256-thread blocks
- * per SM the register budget must allow (2, 3 or 4).  None of them changes
- * which bundles are traced. */
+ * rounding); block_threads: 128 or 256; sort_bands: 1 hands each warp's
+ * emitted bundles to its lanes in ascending absorption coefficient, so rays
+ * traced side by side have similar path lengths (the execution-order part
+ * of the reference's srt band sorting, mc_gpu_noint.cu:1270-1294);
+ * occupancy: resident 256-thread blocks per SM the register budget must
+ * allow (2, 3 or 4).  None of them changes which bundles are traced. */
 int rc_set_launch(rc_ctx *ctx, int rays_per_thread, int block_threads, int sort_bands, int occupancy);
 int rc_get_launch(rc_ctx *ctx, int *rays_per_thread, int *block_threads, int *sort_bands, int *occupancy);
 /* Try launch configurations on T (host) with a reduced bundle count
- * (pilot_photmax) and keep the fastest; writes the chosen knobs. */
+ * (pilot_photmax; <= 0: the context's photmax) and keep the fastest:
+ * rays_per_thread x block_threads x occupancy with sorting off, then
+ * sort_bands on at the best of those.  Writes the chosen knobs. */
 int rc_autotune(rc_ctx *ctx, const float *T, int zstart, int pilot_photmax,
-                int *rays_per_thread, int *block_threads, int *occupancy);
+                int *rays_per_thread, int *block_threads, int *sort_bands, int *occupancy);
 /* Solve without allocating device memory (this entry point has no
  * counterpart in the reference).  For callers that cannot call cudaMalloc
  * while they run -- a time-stepping code whose device memory is owned by
@@ -283,6 +287,12 @@ int rc_server_submit(rc_server *s, const rc_request *req, int64_t *id);
 /* Wait for a request; Q/sigma in the Fortran result layout (may be NULL). */
 int rc_server_wait(rc_server *s, int64_t id, float *Q, float *sigma, rc_result_info *info);
 int rc_server_stats(rc_server *s, double *solves, double *busy_s, double *hbm_in_use);
+/* Tiles (32 work items each) per march launch, shared among the running
+ * requests (default 131072): smaller quanta let new requests start sooner,
+ * larger ones cost fewer launches. */
+int rc_server_set_quantum(rc_server *s, long long tiles);
+/* March launches issued so far. */
+int rc_server_quanta(rc_server *s, long long *quanta);
 int rc_server_destroy(rc_server *s);
 
 /* ---------------- reference-compatible entry points ---------------- */

@@ -111,7 +111,8 @@ _SIGS = [
     ("rc_solve_info_get", _I, [_VP, C.c_int32, C.POINTER(RcSolveInfo)]),
     ("rc_set_launch", _I, [_VP, _I, _I, _I, _I]),
     ("rc_get_launch", _I, [_VP, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int)]),
-    ("rc_autotune", _I, [_VP, _FP, _I, _I, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+    ("rc_autotune", _I, [_VP, _FP, _I, _I, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int),
+                         C.POINTER(C.c_int)]),
     ("rc_solve_noalloc", _I, [_VP, _VP, _I, _VP, _VP, _VP, _VP]),
     ("rc_destroy", _I, [_VP]),
     ("rc_last_error", _I, [_VP, C.c_char_p, C.c_size_t]),
@@ -129,6 +130,8 @@ _SIGS = [
     ("rc_server_wait", _I, [_VP, C.c_int64, _FP, _FP, C.POINTER(RcResultInfo)]),
     ("rc_server_stats", _I, [_VP, _DP, _DP, _DP]),
     ("rc_server_destroy", _I, [_VP]),
+    ("rc_server_set_quantum", _I, [_VP, C.c_longlong]),
+    ("rc_server_quanta", _I, [_VP, C.POINTER(C.c_longlong)]),
     ("rc_legacy_configure", _I, [C.POINTER(RcParams), C.POINTER(RcTables)]),
     ("rc_legacy_release", _I, []),
     ("mc_gpu_", None, [_FP, C.POINTER(C.c_int), C.POINTER(C.c_int)]),

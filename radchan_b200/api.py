@@ -104,6 +104,18 @@ class TableSet:
             pass
 
 
+def rel_std_maxq(q, sigma):
+    """Relative Monte Carlo standard deviation of max|Q|: RMS sigma of the
+    cells whose |Q| is within 10% of the maximum, over max|Q| (the
+    estimator the server uses to meet a tolerance)."""
+    a = np.abs(np.asarray(q, np.float64))
+    best = a.max()
+    if not best > 0:
+        return 0.0
+    m = a >= 0.9 * best
+    return float(np.sqrt(np.mean(np.asarray(sigma, np.float64)[m] ** 2)) / best)
+
+
 def field_shape(p):
     """numpy shape of the temperature field: (kmax+2, jmax+2, imax+2), i fastest."""
     return (p.kmax + 2, p.jmax + 2, p.imax + 2)
@@ -200,11 +212,13 @@ class Solver:
         return list(out), cells[:, :max_cells]
 
     def autotune(self, T, zstart=1, pilot_photmax=16):
+        """Pick rays_per_thread, block_threads, sort_bands and occupancy by
+        timing pilot solves on T; returns the chosen (rpt, block, sort, occupancy)."""
         T = np.ascontiguousarray(T, dtype=np.float32)
-        a, b, c = C.c_int(), C.c_int(), C.c_int()
+        a, b, c, d = C.c_int(), C.c_int(), C.c_int(), C.c_int()
         L.check(L.lib().rc_autotune(self.ctx, T.ctypes.data_as(C.POINTER(C.c_float)), zstart, pilot_photmax,
-                                    C.byref(a), C.byref(b), C.byref(c)), self.ctx)
-        return a.value, b.value, c.value
+                                    C.byref(a), C.byref(b), C.byref(c), C.byref(d)), self.ctx)
+        return a.value, b.value, c.value, d.value
 
     def close(self):
         if self.ctx:
@@ -253,6 +267,10 @@ class Batch:
         dp = lambda a: a.ctypes.data_as(C.POINTER(C.c_double)) if a is not None else None
         L.check(L.lib().rc_batch_collect(self.h, index, fp(Q), fp(S), dp(q64), dp(v64), dp(qw), dp(vw)))
         return Result(Q, S, q64, v64, qw, vw)
+
+    def collect_into(self, index, Q: np.ndarray, S: np.ndarray):
+        fp = lambda a: a.ctypes.data_as(C.POINTER(C.c_float))
+        L.check(L.lib().rc_batch_collect(self.h, index, fp(Q), fp(S), None, None, None, None))
 
     def close(self):
         if self.h:
@@ -321,10 +339,15 @@ class Server:
         L.check(L.lib().rc_server_wait(self.h, rid, fp(Q), fp(S), C.byref(info)))
         return ServedResult(Q, S, info.t_submit, info.t_admit, info.t_done, info.photmax, info.rel_std_maxq)
 
+    def set_quantum(self, tiles: int):
+        L.check(L.lib().rc_server_set_quantum(self.h, int(tiles)))
+
     def stats(self):
         a, b, c = C.c_double(), C.c_double(), C.c_double()
         L.check(L.lib().rc_server_stats(self.h, C.byref(a), C.byref(b), C.byref(c)))
-        return {"solves": a.value, "busy_s": b.value, "hbm_in_use": c.value}
+        q = C.c_longlong()
+        L.check(L.lib().rc_server_quanta(self.h, C.byref(q)))
+        return {"solves": a.value, "busy_s": b.value, "hbm_in_use": c.value, "quanta": q.value}
 
     def close(self):
         if self.h:

@@ -37,6 +37,7 @@ constexpr int kWarp = 32;
 constexpr int kRing = 64;    // per-warp ring of emitted bundles (two waves)
 constexpr int kGuide = 256;  // buckets of the band-CDF guide tables
 constexpr int kFeedIdle = 8; // idle lanes that make a warp leave its step loop to take new bundles
+constexpr int kChunkMax = 8;  // tiles a warp claims per work-queue fetch (guided: fewer near the end)
 
 // ---------------------------------------------------------------------------
 // descriptors
@@ -80,6 +81,7 @@ struct DSolve {
     int wtype[6];
     int nT, nB, nQ;
     int nVar, photmax, rpt, nchunk, gsize, nparts;
+    int sort;  // 1: emitted bundles enter the ring in ascending k (band-sorted order)
     int nwalls, wall_id[2];
     int pad;
     R Lx, Ly, Lz;

@@ -570,6 +570,7 @@ struct Impl : ImplBase {
         d.nVar = p.nVar;
         d.photmax = p.photmax;
         d.rpt = rpt;
+        d.sort = c->sort ? 1 : 0;
         decompose(rpt, d.nchunk, d.gsize, d.nparts);
         d.nwalls = 0;
         if (p.calcwalls) {
@@ -829,66 +830,78 @@ struct Impl : ImplBase {
 
     // Launch-configuration sweep on a reduced bundle count: the knobs do
     // not change the sampled bundles (counter-based draws), only the work
-    // decomposition and the FP64 summation grouping.
-    int autotune(const float *T, int zstart, int pilot, int *rpt_out, int *block_out, int *occ_out) {
+    // decomposition, the FP64 summation grouping and the order in which a
+    // warp's lanes take bundles.
+    int time_config(Slot<R> &s, int zstart, int rpt, int block, int minb, float *ms_out) {
+        std::string *err_ = &c->err;
+        float tot = 0.f;
+        for (int rep = 0; rep < 2; ++rep) {
+            int rc = prepare(s, nullptr, zstart, rpt, s.st);
+            if (rc) return rc;
+            s.h_tiles[0] = 0;
+            s.h_tiles[1] = s.h_desc->n_tiles;
+            RC_CK(cudaMemcpyAsync(s.d_tiles, s.h_tiles, 2 * sizeof(long long), cudaMemcpyHostToDevice, s.st));
+            RC_CK(cudaEventRecord(s.e_march0, s.st));
+            rc = launch_march(s.d_desc, s.d_tiles, 1, s.h_desc->n_tiles, s.d_counter, block, rpt, s.st, minb);
+            if (rc) return rc;
+            RC_CK(cudaEventRecord(s.e_march1, s.st));
+            RC_CK(cudaEventSynchronize(s.e_march1));
+            float ms = 0.f;
+            RC_CK(cudaEventElapsedTime(&ms, s.e_march0, s.e_march1));
+            if (rep > 0) tot += ms;  // the first run warms up
+        }
+        *ms_out = tot;
+        return RC_OK;
+    }
+
+    int autotune(const float *T, int zstart, int pilot, int *rpt_out, int *block_out, int *sort_out, int *occ_out) {
         std::string *err_ = &c->err;
         int rc = check_solve_args(T, zstart);
         if (rc) return rc;
         Slot<R> *sp = free_slot();
         if (!sp) return set_err(err_, RC_E_BUSY, "all solve slots in use");
         Slot<R> &s = *sp;
-        const int saved_photmax = c->p.photmax;
+        const int saved_photmax = c->p.photmax, saved_sort = c->sort;
         if (pilot > 0) c->p.photmax = pilot;
         rc = stage_host_field(s, T);
         float best = 3.4e38f;
-        int brpt = c->rpt, bblock = c->block, bminb = c->minb;
+        int brpt = c->rpt, bblock = c->block, bminb = c->minb, bsort = 0;
         const int rpts[] = {2, 4, 8, 16, 32};
         const int blocks[] = {128, 256};
         const int minbs[] = {2, 3, 4};
+        c->sort = 0;
         for (int oi = 0; oi < 3 && !rc; ++oi)
-        for (int bi = 0; bi < 2 && !rc; ++bi)
-            for (int ri = 0; ri < 5 && !rc; ++ri) {
-                const int rpt = rpts[ri], block = blocks[bi], minb = minbs[oi];
-                if (march_smem(block, rpt) > (size_t)smem_opt_in) continue;
-                float tot = 0.f;
-                for (int rep = 0; rep < 2 && !rc; ++rep) {
-                    rc = prepare(s, nullptr, zstart, rpt, s.st);
-                    if (rc) break;
-                    s.h_tiles[0] = 0;
-                    s.h_tiles[1] = s.h_desc->n_tiles;
-                    cudaError_t e = cudaMemcpyAsync(s.d_tiles, s.h_tiles, 2 * sizeof(long long),
-                                                    cudaMemcpyHostToDevice, s.st);
-                    if (e != cudaSuccess) {
-                        rc = set_err(err_, RC_E_CUDA, cudaGetErrorString(e));
-                        break;
-                    }
-                    cudaEventRecord(s.e_march0, s.st);
-                    rc = launch_march(s.d_desc, s.d_tiles, 1, s.h_desc->n_tiles, s.d_counter, block, rpt, s.st, minb);
-                    if (rc) break;
-                    cudaEventRecord(s.e_march1, s.st);
-                    e = cudaEventSynchronize(s.e_march1);
-                    if (e != cudaSuccess) {
-                        rc = set_err(err_, RC_E_CUDA, cudaGetErrorString(e));
-                        break;
-                    }
+            for (int bi = 0; bi < 2 && !rc; ++bi)
+                for (int ri = 0; ri < 5 && !rc; ++ri) {
+                    const int rpt = rpts[ri], block = blocks[bi], minb = minbs[oi];
+                    if (march_smem(block, rpt) > (size_t)smem_opt_in) continue;
                     float ms = 0.f;
-                    cudaEventElapsedTime(&ms, s.e_march0, s.e_march1);
-                    if (rep > 0) tot += ms;  // first run warms up
+                    rc = time_config(s, zstart, rpt, block, minb, &ms);
+                    if (!rc && ms < best) {
+                        best = ms;
+                        brpt = rpt;
+                        bblock = block;
+                        bminb = minb;
+                    }
                 }
-                if (!rc && tot < best) {
-                    best = tot;
-                    brpt = rpt;
-                    bblock = block;
-                    bminb = minb;
-                }
-            }
+        if (!rc) {
+            c->sort = 1;
+            float ms = 0.f;
+            rc = time_config(s, zstart, brpt, bblock, bminb, &ms);
+            if (!rc && ms < best) bsort = 1;
+        }
         c->p.photmax = saved_photmax;
-        if (rc) return rc;
+        if (rc) {
+            c->sort = saved_sort;
+            return rc;
+        }
         c->rpt = brpt;
         c->block = bblock;
         c->minb = bminb;
+        c->sort = bsort;
         if (rpt_out) *rpt_out = brpt;
         if (block_out) *block_out = bblock;
+        if (sort_out) *sort_out = bsort;
         if (occ_out) *occ_out = bminb;
         return RC_OK;
     }

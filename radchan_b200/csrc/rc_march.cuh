@@ -95,6 +95,10 @@ __global__ void __launch_bounds__(256, MINB) k_march(MarchArgs a) {
     int next_b = 0, head = 0, count = 0;
     bool drained = false;   // no more tiles
     unsigned long long pending = ~0ull;  // fetched tile waiting for a solve switch
+    // tiles claimed from the queue but not started: [chunk_next, chunk_end)
+    unsigned long long chunk_next = 0, chunk_end = 0;
+    const unsigned long long total = (unsigned long long)a.total_tiles;
+    const unsigned long long all_warps = (unsigned long long)gridDim.x * nwarps;
     // lane state
     bool active = false;
     int myb = 0, mypar = 0;
@@ -108,8 +112,25 @@ __global__ void __launch_bounds__(256, MINB) k_march(MarchArgs a) {
             if (!((busy >> fpar) & 1u)) {
                 unsigned long long tile = pending;
                 if (tile == ~0ull) {
-                    if (lane == 0) tile = atomicAdd(a.tile_counter, 1ull);
-                    tile = __shfl_sync(0xffffffffu, tile, 0);
+                    if (chunk_next >= chunk_end) {
+                        // guided self-scheduling: claim up to kChunkMax
+                        // consecutive tiles (usually of one solve), so a warp
+                        // keeps two tiles of the same solve in flight; claim
+                        // fewer as the queue drains to keep the tail short
+                        unsigned long long c0 = 0;
+                        if (lane == 0) {
+                            const unsigned long long seen = *(volatile unsigned long long *)a.tile_counter;
+                            const unsigned long long rem = seen < total ? total - seen : 0ull;
+                            const unsigned long long k =
+                                max(1ull, min((unsigned long long)kChunkMax, rem / (4ull * all_warps)));
+                            c0 = atomicAdd(a.tile_counter, k);
+                            chunk_end = min(c0 + k, total);
+                        }
+                        c0 = __shfl_sync(0xffffffffu, c0, 0);
+                        chunk_end = __shfl_sync(0xffffffffu, chunk_end, 0);
+                        chunk_next = c0;
+                    }
+                    tile = chunk_next < chunk_end ? chunk_next++ : total;
                 }
                 if (tile >= (unsigned long long)a.total_tiles) {
                     drained = true;
@@ -161,7 +182,26 @@ __global__ void __launch_bounds__(256, MINB) k_march(MarchArgs a) {
                 }
             }
             const unsigned m = __ballot_sync(0xffffffffu, ok);
-            if (ok) ws->ring[(head + count + __popc(m & lt)) & (kRing - 1)] = e;
+            int pos = __popc(m & lt);
+            if (S.sort) {
+                // band-sorted order: the wave enters the ring by ascending
+                // k_{nb,g} at the table row nearest Tmax (ties by lane), so
+                // bundles handed out together have similar optical path
+                // lengths.  Which lane traces a bundle does not change its
+                // tally (each bundle owns its slot).
+                unsigned key = 0xffffffffu;
+                if (ok) {
+                    const int nb = e.nbg & 0xfffff, g = e.nbg >> 20;
+                    key = __float_as_uint((float)S.ki[((size_t)nb * S.nQ + g) * S.nT + S.row].k0);  // k >= 0: monotone bits
+                }
+                int rank = 0;
+                for (int q = 0; q < kWarp; ++q) {
+                    const unsigned kq = __shfl_sync(0xffffffffu, key, q);
+                    rank += (kq < key) || (kq == key && q < lane);
+                }
+                pos = rank;
+            }
+            if (ok) ws->ring[(head + count + pos) & (kRing - 1)] = e;
             count += __popc(m);
             if (epar) out1 += __popc(m);
             else out0 += __popc(m);

@@ -15,9 +15,14 @@
 //     remaining tiles of every running request (processor sharing), so a
 //     request that arrives while long solves run joins the next quantum
 //     instead of queueing behind them;
+//   * quanta go round-robin to eight streams, so a quantum's tail (its
+//     longest rays: in near-transparent bands a ray can take up to the last
+//     level's step budget, maxs, tens of milliseconds) overlaps the next
+//     quanta instead of idling the GPU; the prelude of each quantum (set-up
+//     kernels, descriptor copies) is chained by events so it stays ordered;
 //   * the request whose last tiles ran in a quantum gets its tally and the
-//     scalar copy-back right after it on the same stream; two quanta are in
-//     flight at a time, so the host builds the next while the GPU runs one.
+//     scalar copy-back on a separate stream, after every quantum that may
+//     still hold its tiles.
 //
 // Results are bit-identical to the same request solved alone by a context:
 // every bundle's history depends only on (seed, cell, replicate, bundle),
@@ -76,7 +81,7 @@ struct PoolCtx {
     bool busy;
 };
 
-constexpr long long kQuantumTiles = 131072;  // 16.8M bundles at 4 rays per thread
+constexpr long long kQuantumTiles = 131072;  // default quantum: 16.8M bundles at 4 rays per thread
 constexpr long long kMinShare = 4096;
 constexpr int kPilotPhotmax = 64;
 constexpr int kMaxPhotmax = 1 << 20;
@@ -87,6 +92,8 @@ struct rc_server {
     int device = 0;
     double budget = 0;
     int max_inflight = 8;
+    long long quantum_tiles = kQuantumTiles;
+    long long quanta = 0;
     std::vector<TableSet> tables;
     std::mutex mu;
     std::condition_variable cv_work, cv_done;
@@ -100,18 +107,22 @@ struct rc_server {
     double solves_done = 0, busy_s = 0;
     bool stop = false;
     std::thread worker;
-    cudaStream_t st = nullptr;
-    // quantum launch buffers, one set per parity (two quanta in flight)
+    cudaStream_t st = nullptr;  // tallies and result copies
+    // quantum streams and launch buffers, one set per parity
+    static constexpr int kNQ = 8;
+    cudaStream_t qst[kNQ] = {};
     int cap = 0;
-    DSolve<float> *d_solves[2] = {nullptr, nullptr};
-    long long *d_tiles[2] = {nullptr, nullptr};
-    long long *d_base[2] = {nullptr, nullptr};
-    long long *h_tiles[2] = {nullptr, nullptr};
-    long long *h_base[2] = {nullptr, nullptr};
-    unsigned long long *d_counter[2] = {nullptr, nullptr};
-    cudaEvent_t q_start[2] = {nullptr, nullptr}, q_end[2] = {nullptr, nullptr};
-    bool q_used[2] = {false, false};
-    int q_par = 0;
+    DSolve<float> *d_solves[kNQ] = {};
+    long long *d_tiles[kNQ] = {};
+    long long *d_base[kNQ] = {};
+    long long *h_tiles[kNQ] = {};
+    long long *h_base[kNQ] = {};
+    unsigned long long *d_counter[kNQ] = {};
+    cudaEvent_t pre_done[kNQ] = {};  // prelude (set-up, descriptors) of the parity's latest quantum done
+    cudaEvent_t mend[kNQ] = {};      // march of the parity's latest quantum done
+    bool q_used[kNQ] = {};
+    int q_par = 0, last_par = -1;
+    double busy_since = -1.0;
     std::string err;
 };
 
@@ -185,8 +196,8 @@ namespace {
 int grow_quantum_buffers(rc_server *sv, int n) {
     std::string *err_ = &sv->err;
     if (n <= sv->cap) return RC_OK;
-    RC_CK(cudaStreamSynchronize(sv->st));
-    for (int i = 0; i < 2; ++i) {
+    for (int i = 0; i < rc_server::kNQ; ++i) RC_CK(cudaStreamSynchronize(sv->qst[i]));
+    for (int i = 0; i < rc_server::kNQ; ++i) {
         if (sv->d_solves[i]) cudaFree(sv->d_solves[i]);
         if (sv->d_tiles[i]) cudaFree(sv->d_tiles[i]);
         if (sv->d_base[i]) cudaFree(sv->d_base[i]);
@@ -197,7 +208,7 @@ int grow_quantum_buffers(rc_server *sv, int n) {
     }
     sv->cap = 0;
     const int c = std::max(n, 64);
-    for (int i = 0; i < 2; ++i) {
+    for (int i = 0; i < rc_server::kNQ; ++i) {
         RC_CK(cudaMalloc((void **)&sv->d_solves[i], c * sizeof(DSolve<float>)));
         RC_CK(cudaMalloc((void **)&sv->d_tiles[i], (c + 1) * sizeof(long long)));
         RC_CK(cudaMalloc((void **)&sv->d_base[i], c * sizeof(long long)));
@@ -288,13 +299,33 @@ void account_photmax(rc_server *sv, SrvReq *r) {
         }
 }
 
+// Partial-sum array for the stage's photmax, from the stream-ordered
+// allocator: a plain cudaFree would wait for every quantum in flight.  The
+// old array's last users (marches and the tally of the previous stage) have
+// finished: the host saw the tally's event.
+int ensure_partial_async(rc_server *sv, SrvReq *r, cudaStream_t st) {
+    std::string *err_ = &sv->err;
+    Impl<float> &im = *static_cast<Impl<float> *>(r->ctx->impl);
+    Slot<float> &s = *r->slot;
+    const size_t need = im.partial_count(r->ctx->rpt);
+    if (need <= s.partial_cap) return RC_OK;
+    if (s.d_partial) RC_CK(cudaFreeAsync(s.d_partial, st));
+    s.d_partial = nullptr;
+    s.partial_cap = 0;
+    RC_CK(cudaMallocAsync((void **)&s.d_partial, need * sizeof(double), st));
+    s.partial_cap = need;
+    return RC_OK;
+}
+
 // Field copy, set-up kernels and descriptor of the request's current stage.
-int start_stage(rc_server *sv, SrvReq *r) {
+int start_stage(rc_server *sv, SrvReq *r, cudaStream_t st) {
     Impl<float> &im = *static_cast<Impl<float> *>(r->ctx->impl);
     r->ctx->p.photmax = r->photmax;
     r->ctx->p.seed = r->p.seed;
     account_photmax(sv, r);
-    int rc = im.prepare(*r->slot, nullptr, r->zstart, r->ctx->rpt, sv->st);
+    int rc = ensure_partial_async(sv, r, st);
+    if (rc) return rc;
+    rc = im.prepare(*r->slot, nullptr, r->zstart, r->ctx->rpt, st);
     if (rc) return rc;
     r->tiles = r->slot->h_desc->n_tiles;
     r->next_tile = 0;
@@ -302,16 +333,21 @@ int start_stage(rc_server *sv, SrvReq *r) {
     return RC_OK;
 }
 
-// One quantum: a march launch over equal shares of every marching request's
-// remaining tiles, then the tallies of the requests it completes.
+// Prelude and march of one quantum on stream qst[par]: equal shares of every
+// marching request's remaining tiles in one persistent launch.  Set-up work
+// of new stages was enqueued on the same stream just before.
 int run_quantum(rc_server *sv, const std::vector<SrvReq *> &marching, int par) {
     std::string *err_ = &sv->err;
     const int n = (int)marching.size();
-    int rc = grow_quantum_buffers(sv, n);
-    if (rc) return rc;
+    cudaStream_t st = sv->qst[par];
     long long *ht = sv->h_tiles[par], *hb = sv->h_base[par];
     ht[0] = 0;
-    const long long share = std::max<long long>(kQuantumTiles / n, kMinShare);
+    long long share;
+    {
+        std::lock_guard<std::mutex> lk(sv->mu);
+        share = std::max<long long>(sv->quantum_tiles / n, kMinShare);
+        sv->quanta++;
+    }
     int rpt_max = 1;
     for (int i = 0; i < n; ++i) {
         SrvReq *r = marching[i];
@@ -321,22 +357,37 @@ int run_quantum(rc_server *sv, const std::vector<SrvReq *> &marching, int par) {
         r->next_tile += take;
         rpt_max = std::max(rpt_max, r->ctx->rpt);
         RC_CK(cudaMemcpyAsync(sv->d_solves[par] + i, r->slot->d_desc, sizeof(DSolve<float>),
-                              cudaMemcpyDeviceToDevice, sv->st));
+                              cudaMemcpyDeviceToDevice, st));
     }
-    RC_CK(cudaMemcpyAsync(sv->d_tiles[par], ht, (n + 1) * sizeof(long long), cudaMemcpyHostToDevice, sv->st));
-    RC_CK(cudaMemcpyAsync(sv->d_base[par], hb, n * sizeof(long long), cudaMemcpyHostToDevice, sv->st));
-    k_set_tile_base<<<(n + 127) / 128, 128, 0, sv->st>>>(sv->d_solves[par], sv->d_base[par], n);
+    RC_CK(cudaMemcpyAsync(sv->d_tiles[par], ht, (n + 1) * sizeof(long long), cudaMemcpyHostToDevice, st));
+    RC_CK(cudaMemcpyAsync(sv->d_base[par], hb, n * sizeof(long long), cudaMemcpyHostToDevice, st));
+    k_set_tile_base<<<(n + 127) / 128, 128, 0, st>>>(sv->d_solves[par], sv->d_base[par], n);
     RC_CK(cudaGetLastError());
+    RC_CK(cudaEventRecord(sv->pre_done[par], st));
     if (ht[n] > 0) {
         Impl<float> &im0 = *static_cast<Impl<float> *>(marching[0]->ctx->impl);
-        rc = im0.launch_march(sv->d_solves[par], sv->d_tiles[par], n, ht[n], sv->d_counter[par],
-                              marching[0]->ctx->block, rpt_max, sv->st);
+        const int rc = im0.launch_march(sv->d_solves[par], sv->d_tiles[par], n, ht[n], sv->d_counter[par],
+                                        marching[0]->ctx->block, rpt_max, st);
         if (rc) return set_err(err_, rc, marching[0]->ctx->err);
     }
+    RC_CK(cudaEventRecord(sv->mend[par], st));
+    return RC_OK;
+}
+
+// Tallies of the requests whose last tiles were just issued, on the tally
+// stream after every quantum in flight (any of them may hold their tiles).
+int enqueue_tallies(rc_server *sv, const std::vector<SrvReq *> &marching) {
+    std::string *err_ = &sv->err;
+    bool waited = false;
     for (SrvReq *r : marching) {
         if (r->next_tile < r->tiles) continue;
+        if (!waited) {
+            for (int q = 0; q < rc_server::kNQ; ++q)
+                if (sv->q_used[q]) RC_CK(cudaStreamWaitEvent(sv->st, sv->mend[q], 0));
+            waited = true;
+        }
         Impl<float> &im = *static_cast<Impl<float> *>(r->ctx->impl);
-        rc = im.launch_tally(r->slot->d_desc, r->slot->d_out, 1, im.tally_cells(), sv->st);
+        int rc = im.launch_tally(r->slot->d_desc, r->slot->d_out, 1, im.tally_cells(), sv->st);
         if (rc) return set_err(err_, rc, r->ctx->err);
         RC_CK(cudaMemcpyAsync(r->slot->h_sc, r->slot->d_sc, sizeof(DScalars), cudaMemcpyDeviceToHost, sv->st));
         RC_CK(cudaEventRecord(r->ev, sv->st));
@@ -355,8 +406,9 @@ void finish_stage(rc_server *sv, SrvReq *r) {
         return;
     }
     if (r->stage == ST_PILOT) {
-        if (cudaMemcpy(s.h_Qc, s.d_Qc, ncf * sizeof(float), cudaMemcpyDeviceToHost) != cudaSuccess ||
-            cudaMemcpy(s.h_Sc, s.d_Sc, ncf * sizeof(float), cudaMemcpyDeviceToHost) != cudaSuccess) {
+        if (cudaMemcpyAsync(s.h_Qc, s.d_Qc, ncf * sizeof(float), cudaMemcpyDeviceToHost, s.st) != cudaSuccess ||
+            cudaMemcpyAsync(s.h_Sc, s.d_Sc, ncf * sizeof(float), cudaMemcpyDeviceToHost, s.st) != cudaSuccess ||
+            cudaStreamSynchronize(s.st) != cudaSuccess) {
             fail(sv, r, RC_E_CUDA, "pilot copy failed");
             return;
         }
@@ -430,6 +482,12 @@ void admit(rc_server *sv) {
     }
 }
 
+bool quanta_in_flight(rc_server *sv) {
+    for (int q = 0; q < rc_server::kNQ; ++q)
+        if (sv->q_used[q] && cudaEventQuery(sv->mend[q]) != cudaSuccess) return true;
+    return false;
+}
+
 void worker_loop(rc_server *sv) {
     cudaSetDevice(sv->device);
     for (;;) {
@@ -439,13 +497,13 @@ void worker_loop(rc_server *sv) {
         }
         admit(sv);
         const int par = sv->q_par;
-        // the quantum issued two iterations ago used this parity's buffers
-        if (sv->q_used[par]) {
-            cudaEventSynchronize(sv->q_end[par]);
-            float ms = 0.f;
-            cudaEventElapsedTime(&ms, sv->q_start[par], sv->q_end[par]);
-            sv->busy_s += ms * 1e-3;
-            sv->q_used[par] = false;
+        // at most kNQ quanta in flight: this parity's previous quantum must
+        // have finished before its stream and buffers take the next one
+        if (sv->q_used[par]) cudaEventSynchronize(sv->mend[par]);
+        if (sv->busy_since >= 0 && !quanta_in_flight(sv)) {
+            std::lock_guard<std::mutex> lk(sv->mu);
+            sv->busy_s += now_s() - sv->busy_since;
+            sv->busy_since = -1.0;
         }
         // completed tallies
         bool progressed = false;
@@ -454,32 +512,49 @@ void worker_loop(rc_server *sv) {
                 finish_stage(sv, r);
                 progressed = true;
             }
-        // set-up of ready stages and one quantum over every marching request
-        std::vector<SrvReq *> marching;
-        bool tallying = false;
-        cudaEventRecord(sv->q_start[par], sv->st);
+        bool prepare = false, tallying = false;
+        int n_march = 0;
         for (SrvReq *r : sv->running) {
             if (r->stage >= ST_DONE) continue;
-            if (r->phase == PH_PREPARE) {
-                const int rc = start_stage(sv, r);
-                if (rc) {
-                    fail(sv, r, rc, r->ctx ? r->ctx->err : g_err);
-                    continue;
+            prepare |= r->phase == PH_PREPARE;
+            n_march += r->phase != PH_TALLY;
+            tallying |= r->phase == PH_TALLY;
+        }
+        std::vector<SrvReq *> marching;
+        if (n_march > 0) {
+            cudaStream_t st = sv->qst[par];
+            int rc = grow_quantum_buffers(sv, n_march);
+            // the prelude follows the previous quantum's prelude
+            if (!rc && sv->last_par >= 0) rc = cudaStreamWaitEvent(st, sv->pre_done[sv->last_par], 0) ? RC_E_CUDA : 0;
+            if (rc) {
+                for (SrvReq *r : sv->running)
+                    if (r->stage < ST_DONE && r->phase != PH_TALLY) fail(sv, r, rc, sv->err);
+            } else {
+                if (prepare)
+                    for (SrvReq *r : sv->running) {
+                        if (r->stage >= ST_DONE || r->phase != PH_PREPARE) continue;
+                        const int e = start_stage(sv, r, st);
+                        if (e) fail(sv, r, e, r->ctx ? r->ctx->err : g_err);
+                    }
+                for (SrvReq *r : sv->running)
+                    if (r->stage < ST_DONE && r->phase == PH_MARCH) marching.push_back(r);
+                if (!marching.empty()) {
+                    if (sv->busy_since < 0) sv->busy_since = now_s();
+                    rc = run_quantum(sv, marching, par);
+                    if (!rc) {
+                        sv->q_used[par] = true;
+                        sv->last_par = par;
+                        sv->q_par = (par + 1) % rc_server::kNQ;
+                        rc = enqueue_tallies(sv, marching);
+                    }
+                    if (rc) {
+                        for (int q = 0; q < rc_server::kNQ; ++q) cudaStreamSynchronize(sv->qst[q]);
+                        cudaStreamSynchronize(sv->st);
+                        for (SrvReq *r : marching) fail(sv, r, rc, sv->err);
+                    }
                 }
             }
-            if (r->phase == PH_MARCH) marching.push_back(r);
-            if (r->phase == PH_TALLY) tallying = true;
         }
-        if (!marching.empty()) {
-            const int rc = run_quantum(sv, marching, par);
-            if (rc) {
-                cudaStreamSynchronize(sv->st);
-                for (SrvReq *r : marching) fail(sv, r, rc, sv->err);
-            }
-        }
-        cudaEventRecord(sv->q_end[par], sv->st);
-        sv->q_used[par] = true;
-        sv->q_par ^= 1;
         {
             std::lock_guard<std::mutex> lk(sv->mu);
             std::vector<SrvReq *> keep;
@@ -498,7 +573,7 @@ void worker_loop(rc_server *sv) {
         if (marching.empty()) {
             if (tallying) {
                 cudaStreamSynchronize(sv->st);
-            } else {
+            } else if (!progressed) {
                 std::unique_lock<std::mutex> lk(sv->mu);
                 if (sv->running.empty())
                     sv->cv_work.wait_for(lk, std::chrono::milliseconds(5),
@@ -506,6 +581,7 @@ void worker_loop(rc_server *sv) {
             }
         }
     }
+    for (int q = 0; q < rc_server::kNQ; ++q) cudaStreamSynchronize(sv->qst[q]);
     cudaStreamSynchronize(sv->st);
     // requests still queued or running end as failed
     std::lock_guard<std::mutex> lk(sv->mu);
@@ -536,9 +612,11 @@ int rc_server_create(int device, double hbm_budget_bytes, int max_inflight, rc_s
     sv->budget = hbm_budget_bytes > 0 ? hbm_budget_bytes : 150e9;
     sv->max_inflight = max_inflight;
     bool ok = cudaStreamCreateWithFlags(&sv->st, cudaStreamNonBlocking) == cudaSuccess;
-    for (int i = 0; i < 2 && ok; ++i)
-        ok = cudaMalloc((void **)&sv->d_counter[i], sizeof(unsigned long long)) == cudaSuccess &&
-             cudaEventCreate(&sv->q_start[i]) == cudaSuccess && cudaEventCreate(&sv->q_end[i]) == cudaSuccess;
+    for (int i = 0; i < rc_server::kNQ && ok; ++i)
+        ok = cudaStreamCreateWithFlags(&sv->qst[i], cudaStreamNonBlocking) == cudaSuccess &&
+             cudaMalloc((void **)&sv->d_counter[i], sizeof(unsigned long long)) == cudaSuccess &&
+             cudaEventCreateWithFlags(&sv->pre_done[i], cudaEventDisableTiming) == cudaSuccess &&
+             cudaEventCreateWithFlags(&sv->mend[i], cudaEventDisableTiming) == cudaSuccess;
     if (!ok) {
         rc_server_destroy(sv);
         return set_err(nullptr, RC_E_CUDA, "server stream/event creation failed");
@@ -620,6 +698,21 @@ int rc_server_wait(rc_server *sv, int64_t id, float *Q, float *sigma, rc_result_
     return RC_OK;
 }
 
+int rc_server_set_quantum(rc_server *sv, long long tiles) {
+    if (!sv) return set_err(nullptr, RC_E_INVALID, "NULL server");
+    if (tiles < 1) return set_err(nullptr, RC_E_INVALID, "quantum must be >= 1 tile");
+    std::lock_guard<std::mutex> lk(sv->mu);
+    sv->quantum_tiles = tiles;
+    return RC_OK;
+}
+
+int rc_server_quanta(rc_server *sv, long long *quanta) {
+    if (!sv || !quanta) return set_err(nullptr, RC_E_INVALID, "NULL argument");
+    std::lock_guard<std::mutex> lk(sv->mu);
+    *quanta = sv->quanta;
+    return RC_OK;
+}
+
 int rc_server_stats(rc_server *sv, double *solves, double *busy_s, double *hbm_in_use) {
     if (!sv) return set_err(nullptr, RC_E_INVALID, "NULL server");
     std::lock_guard<std::mutex> lk(sv->mu);
@@ -638,19 +731,22 @@ int rc_server_destroy(rc_server *sv) {
     }
     if (sv->worker.joinable()) sv->worker.join();
     cudaSetDevice(sv->device);
+    for (int i = 0; i < rc_server::kNQ; ++i)
+        if (sv->qst[i]) cudaStreamSynchronize(sv->qst[i]);
     if (sv->st) cudaStreamSynchronize(sv->st);
     for (auto &pc : sv->pool) rc_destroy(pc.ctx);
     for (auto &kv : sv->reqs)
         if (kv.second->ev) cudaEventDestroy(kv.second->ev);
-    for (int i = 0; i < 2; ++i) {
+    for (int i = 0; i < rc_server::kNQ; ++i) {
         if (sv->d_solves[i]) cudaFree(sv->d_solves[i]);
         if (sv->d_tiles[i]) cudaFree(sv->d_tiles[i]);
         if (sv->d_base[i]) cudaFree(sv->d_base[i]);
         if (sv->h_tiles[i]) cudaFreeHost(sv->h_tiles[i]);
         if (sv->h_base[i]) cudaFreeHost(sv->h_base[i]);
         if (sv->d_counter[i]) cudaFree(sv->d_counter[i]);
-        if (sv->q_start[i]) cudaEventDestroy(sv->q_start[i]);
-        if (sv->q_end[i]) cudaEventDestroy(sv->q_end[i]);
+        if (sv->pre_done[i]) cudaEventDestroy(sv->pre_done[i]);
+        if (sv->mend[i]) cudaEventDestroy(sv->mend[i]);
+        if (sv->qst[i]) cudaStreamDestroy(sv->qst[i]);
     }
     if (sv->st) cudaStreamDestroy(sv->st);
     delete sv;

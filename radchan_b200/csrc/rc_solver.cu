@@ -359,11 +359,11 @@ void batch_release(rc_batch *b) {
 extern "C" {
 
 int rc_autotune(rc_ctx *c, const float *T, int zstart, int pilot_photmax, int *rays_per_thread, int *block_threads,
-                int *sort_bands) {
+                int *sort_bands, int *occupancy) {
     if (!c) return set_err(nullptr, RC_E_INVALID, "NULL context");
     cudaSetDevice(c->device);
     return with_impl(c, [&](auto &im) {
-        return im.autotune(T, zstart, pilot_photmax, rays_per_thread, block_threads, sort_bands);
+        return im.autotune(T, zstart, pilot_photmax, rays_per_thread, block_threads, sort_bands, occupancy);
     });
 }
 

@@ -1,0 +1,51 @@
+"""Launch knobs and the autotuner: block size, occupancy and the band-sorted
+bundle order change neither the traced bundles nor the result; the rays per
+thread fix the FP64 summation grouping, so results equal the oracle run with
+the same grouping."""
+import numpy as np
+import pytest
+
+from radchan_b200 import api
+from radchan_b200 import workloads as W
+
+pytestmark = pytest.mark.gpu
+
+
+def _nb_case():
+    tabs = W.tables_nb(nB=40, nQ=4, nT=32)
+    p = W.channel_params(32, 16, 16, photmax=64, nVar=4, nB=40, nQ=4, nT=32,
+                         levels=[(32, 16, 16), (16, 8, 8)], maxs=[5, 100000], calcwalls=1, adiabw=1)
+    return p, tabs, W.channel_field(p, seed=21)
+
+
+@pytest.mark.parametrize("grey", [True, False])
+def test_sort_block_occupancy_leave_result_unchanged(grey):
+    if grey:
+        p, tabs, T = W.config_grey_32(photmax=64), None, W.channel_field(W.config_grey_32(), seed=3)
+    else:
+        p, tabs, T = _nb_case()
+    s = api.Solver(p, tabs)
+    s.set_launch(rays_per_thread=4, block_threads=256, sort_bands=0, occupancy=4)
+    base = s.solve(T)
+    for block, sort, occ in ((256, 1, 4), (128, 1, 2), (128, 0, 3)):
+        s.set_launch(rays_per_thread=4, block_threads=block, sort_bands=sort, occupancy=occ)
+        assert s.get_launch() == (4, block, sort, occ)
+        r = s.solve(T)
+        np.testing.assert_array_equal(r.q64, base.q64)
+        np.testing.assert_array_equal(r.var64, base.var64)
+        np.testing.assert_array_equal(r.qw64, base.qw64)
+    s.close()
+
+
+def test_autotune_picks_valid_knobs_and_matches_oracle():
+    from oracle import oracle as O
+    p, tabs, T = _nb_case()
+    s = api.Solver(p, tabs)
+    rpt, block, sort, occ = s.autotune(T, pilot_photmax=0)
+    assert rpt in (2, 4, 8, 16, 32) and block in (128, 256) and sort in (0, 1) and occ in (2, 3, 4)
+    assert s.get_launch() == (rpt, block, sort, occ)
+    r = s.solve(T)
+    o = O.solve(p, tabs, T, rpt=rpt)
+    np.testing.assert_array_equal(r.q64, o["q64"])
+    np.testing.assert_array_equal(r.var64, o["var64"])
+    s.close()
