@@ -22,7 +22,8 @@ Legs on one GPU (skipped with --no-legs):
          continuous-batching server, solves/s by wall clock.
 
 --serve runs the open-loop serving benchmark instead (Poisson arrivals at
---load x measured capacity, tolerance-driven photmax, p50/p99 latency).
+--load x measured capacity, tolerance-driven photmax, p50/p99 latency);
+--precision runs the FP32-march vs FP64-build study at 192x128x128.
 
 --impl reference times the CPU restatement of the reference's ray loop
 (the reference has no CPU implementation of this path) on all host cores.
@@ -43,6 +44,12 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 BUNDLE_METRIC = "bundles/s & solves/s at 1% MC std, batched/served vs plain; serve p50/p99"
+
+# DRAM bytes (read + write) of one k_march launch, from the ncu capture
+# summarised in profiles/k_march_nb64_photmax64_full.txt
+# (dram__bytes_read.sum + dram__bytes_write.sum).  The march's working set (temperature pyramid and
+# tables, ~1.5 MB) is L2-resident, so the traffic does not grow with photmax.
+K_MARCH_TRAFFIC = {"nb64": 994304 + 4096}
 
 
 def peaks():
@@ -321,7 +328,8 @@ def run_serve(args, rank, local):
     256x128x128 (eight size classes), tolerance drawn log-uniformly from
     1% to 5% relative std of max|Q| (photmax chosen by the server), fields
     and tables resident, admission by a 150 GB budget.  The arrival rate is
-    args.load x the capacity measured with a closed burst of the same mix."""
+    args.load x the capacity 1 / E[service time alone] of the mix, with the
+    service time of every size class measured alone after calibration."""
     if rank != 0:
         return
     import threading
@@ -340,6 +348,7 @@ def run_serve(args, rank, local):
                              maxs=[5, 5, 100000], calcwalls=1, adiabw=1)
         classes.append((p, W.channel_field(p, seed=100 + c)))
     srv = api.Server(device=local, hbm_budget_bytes=150e9, max_inflight=args.serve_inflight)
+    srv.set_policy(args.policy)
     ts = srv.add_tables(tabs)
 
     def draw(n):
@@ -357,14 +366,13 @@ def run_serve(args, rank, local):
         srv.wait(srv.submit(p, T, table_set=ts, tolerance=0.03))
         r = srv.wait(srv.submit(p, T, table_set=ts, tolerance=0.03))
         alone.append((r.t_done - r.t_admit, r.photmax))
-    burst = draw(args.serve_burst)
-    t0 = time.perf_counter()
-    ids = [srv.submit(classes[c][0], classes[c][1], table_set=ts, tolerance=tol) for c, tol in burst]
-    for rid in ids:
-        srv.wait(rid)
-    cap = len(burst) / (time.perf_counter() - t0)
-    rate = args.load * cap
+    # capacity: one over the mean service time alone of the request mix
+    # (photmax grows as 1/tol^2 from the 3% calibration); concurrent small
+    # requests share the GPU better than that, so the load is conservative
     reqs = draw(args.serve_requests)
+    mean_svc = float(np.mean([alone[c][0] * (0.03 / tol) ** 2 for c, tol in reqs]))
+    cap = 1.0 / mean_svc
+    rate = args.load * cap
     gaps = rng.exponential(1.0 / rate, size=len(reqs))
     results = [None] * len(reqs)
     ids = [None] * len(reqs)
@@ -397,7 +405,7 @@ def run_serve(args, rank, local):
     slow = lat / svc
     met = np.array([r.rel_std_maxq <= 1.25 * tol for r, (_, tol) in zip(results, reqs)])
     line = {"metric": "serve latency p50/p99 and solves/s", "impl": "ours", "n_gpus": 1,
-            "requests": len(reqs), "load": args.load, "capacity_solves_per_s": cap,
+            "requests": len(reqs), "load": args.load, "capacity_solves_per_s": cap, "policy": args.policy,
             "offered_solves_per_s": rate, "solves_per_s": len(reqs) / wall,
             "p50_s": float(np.percentile(lat, 50)), "p99_s": float(np.percentile(lat, 99)),
             "p99_over_p50": float(np.percentile(lat, 99) / np.percentile(lat, 50)),
@@ -411,7 +419,40 @@ def run_serve(args, rank, local):
             "config": {"workload": "Poisson stream, narrow-band 100x8, grids 32^3..256x128x128 in 8 log-spaced "
                                    "classes, tolerance 1-5% log-uniform, 150 GB budget",
                        "classes": [[p.imax, p.jmax, p.kmax] for p, _ in classes],
-                       "max_inflight": args.serve_inflight, "burst": len(burst)}}
+                       "max_inflight": args.serve_inflight}}
+    print(json.dumps(line), flush=True)
+
+
+def run_precision(args, rank, local):
+    """Precision study: 192x128x128, optically thick tables (log10 k0 in
+    [-1, 2]), emissivity 0.8, specular y walls, adiabatic x walls with wall
+    fluxes, photmax 1024, nVar 8.  The FP32 march with FP64 tally against the
+    full-FP64 build with identical Philox streams; per-cell and wall-flux
+    differences in units of the Monte Carlo standard deviation."""
+    if rank != 0:
+        return
+    from radchan_b200 import api
+    from radchan_b200 import workloads as W
+    tabs = W.tables_nb(logk_lo=-1.0, logk_hi=2.0)
+    p32 = W.config_precision(photmax=args.photmax or 1024)
+    p64 = api.copy_params(p32)
+    p64.floatpoint = 1
+    T = W.channel_field(p32, seed=11)
+    out = {}
+    res = {}
+    for name, p in (("fp32", p32), ("fp64", p64)):
+        s = api.Solver(p, tabs, device=local)
+        t = s.solve_async(T)
+        info = s.info(t)
+        res[name] = s.collect(t)
+        out[name] = {"ms_solve": info.ms_solve, "bundles_per_s": info.bundles / (info.ms_solve / 1000.0),
+                     "rel_std_maxq": api.rel_std_maxq(res[name].q64, np.sqrt(res[name].var64))}
+        s.close()
+    line = {"metric": "FP32 march vs FP64 build, error in MC standard deviations", "impl": "ours", "n_gpus": 1,
+            "data": "synthetic", "runs": out, "error_in_sigma": api.compare_in_sigma(res["fp32"], res["fp64"]),
+            "fp64_over_fp32_time": out["fp64"]["ms_solve"] / out["fp32"]["ms_solve"],
+            "config": {"workload": "192x128x128 narrow-band 100x8, log10 k0 in [-1,2], eps 0.8, specular y, "
+                                   "adiabatic x walls with fluxes, photmax %d, nVar 8" % p32.photmax}}
     print(json.dumps(line), flush=True)
 
 
@@ -480,8 +521,9 @@ def run_ours(args, ws, rank, local):
     peak, peak_kind = peaks()
     march_s = sum(ms_march) / 1000.0
     achieved = steps * 32.0 / march_s / 1e9
+    traffic = args.traffic if args.traffic is not None else K_MARCH_TRAFFIC.get(args.workload)
     roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-            "traffic": args.traffic, "kernel": "k_march", "peak_source": peak_kind,
+            "traffic": traffic, "kernel": "k_march", "peak_source": peak_kind,
             "algorithmic_bytes_per_step": 32, "steps_per_launch": steps / args.steps}
     line = {"metric": BUNDLE_METRIC, "value": value, "unit": "bundles/s", "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": 1000 * t_max / args.steps, "higher_is_better": True,
@@ -522,14 +564,17 @@ def main():
     ap.add_argument("--no-legs", dest="no_legs", action="store_true",
                     help="skip the 1%%-tolerance and batched-mix legs (profiling runs)")
     ap.add_argument("--serve", action="store_true", help="open-loop serving run instead of the solve benchmark")
+    ap.add_argument("--precision", action="store_true", help="FP32 march vs FP64 build study instead")
     ap.add_argument("--serve-requests", dest="serve_requests", type=int, default=200)
-    ap.add_argument("--serve-burst", dest="serve_burst", type=int, default=40)
-    ap.add_argument("--serve-inflight", dest="serve_inflight", type=int, default=8)
+    ap.add_argument("--serve-inflight", dest="serve_inflight", type=int, default=32)
+    ap.add_argument("--policy", default="srpt", choices=["srpt", "fair"])
     ap.add_argument("--load", type=float, default=0.8)
     args = ap.parse_args()
     ws, rank, local = dist_init()
     if args.serve:
         run_serve(args, rank, local)
+    elif args.precision:
+        run_precision(args, rank, local)
     elif args.impl == "reference":
         run_reference(args, ws, rank)
     else:

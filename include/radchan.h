@@ -293,6 +293,13 @@ int rc_server_stats(rc_server *s, double *solves, double *busy_s, double *hbm_in
 int rc_server_set_quantum(rc_server *s, long long tiles);
 /* March launches issued so far. */
 int rc_server_quanta(rc_server *s, long long *quanta);
+/* How a quantum's tiles are shared among the running requests:
+ * RC_SCHED_SRPT (default) serves the requests with the least remaining
+ * work first, above a floor of 1/8 of the quantum shared by all;
+ * RC_SCHED_FAIR gives every request an equal share. */
+#define RC_SCHED_FAIR 0
+#define RC_SCHED_SRPT 1
+int rc_server_set_policy(rc_server *s, int policy);
 int rc_server_destroy(rc_server *s);
 
 /* ---------------- reference-compatible entry points ---------------- */

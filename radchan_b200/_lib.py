@@ -132,6 +132,7 @@ _SIGS = [
     ("rc_server_destroy", _I, [_VP]),
     ("rc_server_set_quantum", _I, [_VP, C.c_longlong]),
     ("rc_server_quanta", _I, [_VP, C.POINTER(C.c_longlong)]),
+    ("rc_server_set_policy", _I, [_VP, _I]),
     ("rc_legacy_configure", _I, [C.POINTER(RcParams), C.POINTER(RcTables)]),
     ("rc_legacy_release", _I, []),
     ("mc_gpu_", None, [_FP, C.POINTER(C.c_int), C.POINTER(C.c_int)]),

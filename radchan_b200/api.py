@@ -116,6 +116,25 @@ def rel_std_maxq(q, sigma):
     return float(np.sqrt(np.mean(np.asarray(sigma, np.float64)[m] ** 2)) / best)
 
 
+def compare_in_sigma(a: "Result", b: "Result"):
+    """Per-cell and wall-flux differences of two solves of the same problem
+    (e.g. the FP32 march and the FP64 build with the same streams) in units
+    of the Monte Carlo standard deviation of b."""
+    out = {}
+    for name, q0, q1, v1 in (("cells", a.q64, b.q64, b.var64), ("walls", a.qw64, b.qw64, b.vw64)):
+        q0 = np.asarray(q0, np.float64).ravel()
+        q1 = np.asarray(q1, np.float64).ravel()
+        s = np.sqrt(np.asarray(v1, np.float64).ravel())
+        m = s > 0
+        if not m.any():
+            continue
+        z = (q0[m] - q1[m]) / s[m]
+        out[name] = {"n": int(m.sum()), "max_abs_z": float(np.abs(z).max()), "rms_z": float(np.sqrt(np.mean(z * z))),
+                     "mean_z": float(z.mean()),
+                     "max_rel": float(np.max(np.abs(q0[m] - q1[m]) / np.maximum(np.abs(q1[m]), 1e-300)))}
+    return out
+
+
 def field_shape(p):
     """numpy shape of the temperature field: (kmax+2, jmax+2, imax+2), i fastest."""
     return (p.kmax + 2, p.jmax + 2, p.imax + 2)
@@ -341,6 +360,10 @@ class Server:
 
     def set_quantum(self, tiles: int):
         L.check(L.lib().rc_server_set_quantum(self.h, int(tiles)))
+
+    def set_policy(self, policy: str):
+        """'srpt' (least remaining work first, default) or 'fair' (equal shares)."""
+        L.check(L.lib().rc_server_set_policy(self.h, {"fair": 0, "srpt": 1}[policy]))
 
     def stats(self):
         a, b, c = C.c_double(), C.c_double(), C.c_double()

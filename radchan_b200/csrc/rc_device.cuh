@@ -15,9 +15,11 @@
 //     radchan_math.h;
 //   * face distance ds = (face - p) * (1/s), the reciprocal formed once per
 //     direction change;
-//   * table coordinate p = clamp((T - T0) * (1/dT), 0, nT-1), stored per cell
-//     of every multigrid level; v = col[i0]*(1-a) + col[i1]*a with i0 = (int)p,
-//     a = p - i0;
+//   * table coordinate q = rint(256 * clamp((T - T0) * (1/dT), 0, nT-1)),
+//     8 fractional bits (the weight precision of the texture unit the
+//     reference interpolates with), stored as uint16 per cell of every
+//     multigrid level; v = col[i0]*(1-a) + col[i1]*a with i0 = q >> 8,
+//     i1 = min(i0 + 1, nT - 1), a = (q & 255) / 256;
 //   * alpha = -expm1(-(ds*k)), tra *= (1 + expm1(-(ds*k)));
 //   * step tally c = (((Ibmax*tra)*alpha)*ratioI)*(invTi4*Ib - 1) in the
 //     march precision, accumulated into an FP64 bundle sum;

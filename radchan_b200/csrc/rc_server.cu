@@ -11,10 +11,11 @@
 //     grid, tables and buffers stay resident between requests of the same
 //     problem class (everything but photmax and the seed equal);
 //   * one scheduler thread drives the GPU in quanta: a quantum is one
-//     persistent march launch whose work queue holds an equal share of the
-//     remaining tiles of every running request (processor sharing), so a
-//     request that arrives while long solves run joins the next quantum
-//     instead of queueing behind them;
+//     persistent march launch whose work queue holds tiles of every running
+//     request -- by default the requests with the least remaining work
+//     first, above a floor share for everyone (or equal shares, processor
+//     sharing) -- so a request that arrives while long solves run joins the
+//     next quantum instead of queueing behind them;
 //   * quanta go round-robin to eight streams, so a quantum's tail (its
 //     longest rays: in near-transparent bands a ray can take up to the last
 //     level's step budget, maxs, tens of milliseconds) overlaps the next
@@ -93,6 +94,7 @@ struct rc_server {
     double budget = 0;
     int max_inflight = 8;
     long long quantum_tiles = kQuantumTiles;
+    int policy = RC_SCHED_SRPT;
     long long quanta = 0;
     std::vector<TableSet> tables;
     std::mutex mu;
@@ -342,19 +344,45 @@ int run_quantum(rc_server *sv, const std::vector<SrvReq *> &marching, int par) {
     cudaStream_t st = sv->qst[par];
     long long *ht = sv->h_tiles[par], *hb = sv->h_base[par];
     ht[0] = 0;
-    long long share;
+    long long qt;
+    int policy;
     {
         std::lock_guard<std::mutex> lk(sv->mu);
-        share = std::max<long long>(sv->quantum_tiles / n, kMinShare);
+        qt = sv->quantum_tiles;
+        policy = sv->policy;
         sv->quanta++;
+    }
+    std::vector<long long> take(n, 0);
+    if (policy == RC_SCHED_FAIR) {
+        const long long share = std::max<long long>(qt / n, kMinShare);
+        for (int i = 0; i < n; ++i) take[i] = std::min(share, marching[i]->tiles - marching[i]->next_tile);
+    } else {
+        // shortest remaining work first, with a floor of 1/8 of the quantum
+        // shared by everyone so that long requests keep progressing
+        long long budget = std::max(qt, kMinShare);
+        const long long floor = std::max<long long>(budget / (8LL * n), 1);
+        for (int i = 0; i < n; ++i) {
+            take[i] = std::min(floor, marching[i]->tiles - marching[i]->next_tile);
+            budget -= take[i];
+        }
+        std::vector<int> order(n);
+        for (int i = 0; i < n; ++i) order[i] = i;
+        std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
+            return marching[a]->tiles - marching[a]->next_tile < marching[b]->tiles - marching[b]->next_tile;
+        });
+        for (int i : order) {
+            if (budget <= 0) break;
+            const long long more = std::min(budget, marching[i]->tiles - marching[i]->next_tile - take[i]);
+            take[i] += more;
+            budget -= more;
+        }
     }
     int rpt_max = 1;
     for (int i = 0; i < n; ++i) {
         SrvReq *r = marching[i];
-        const long long take = std::min(share, r->tiles - r->next_tile);
         hb[i] = r->next_tile;
-        ht[i + 1] = ht[i] + take;
-        r->next_tile += take;
+        ht[i + 1] = ht[i] + take[i];
+        r->next_tile += take[i];
         rpt_max = std::max(rpt_max, r->ctx->rpt);
         RC_CK(cudaMemcpyAsync(sv->d_solves[par] + i, r->slot->d_desc, sizeof(DSolve<float>),
                               cudaMemcpyDeviceToDevice, st));
@@ -703,6 +731,14 @@ int rc_server_set_quantum(rc_server *sv, long long tiles) {
     if (tiles < 1) return set_err(nullptr, RC_E_INVALID, "quantum must be >= 1 tile");
     std::lock_guard<std::mutex> lk(sv->mu);
     sv->quantum_tiles = tiles;
+    return RC_OK;
+}
+
+int rc_server_set_policy(rc_server *sv, int policy) {
+    if (!sv) return set_err(nullptr, RC_E_INVALID, "NULL server");
+    if (policy != RC_SCHED_FAIR && policy != RC_SCHED_SRPT) return set_err(nullptr, RC_E_INVALID, "unknown policy");
+    std::lock_guard<std::mutex> lk(sv->mu);
+    sv->policy = policy;
     return RC_OK;
 }
 
