@@ -464,8 +464,9 @@ def run_ours(args, ws, rank, local):
     dev = local
     torch.cuda.set_device(dev)
     s = api.Solver(p, tabs, device=dev)
-    if args.rays_per_thread or args.block or args.occupancy:
-        s.set_launch(rays_per_thread=args.rays_per_thread, block_threads=args.block, occupancy=args.occupancy)
+    if args.rays_per_thread or args.block or args.occupancy or args.sort >= 0:
+        s.set_launch(rays_per_thread=args.rays_per_thread, block_threads=args.block, sort_bands=args.sort,
+                     occupancy=args.occupancy)
     T_dev = torch.from_numpy(T).to(f"cuda:{dev}")
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=f"cuda:{dev}")
     # k_init_scalars, k_tmax, k_setup1, k_setup2, k_levels, k_patch_desc,
@@ -557,6 +558,7 @@ def main():
     ap.add_argument("--rays-per-thread", dest="rays_per_thread", type=int, default=0)
     ap.add_argument("--block", type=int, default=0)
     ap.add_argument("--occupancy", type=int, default=0)
+    ap.add_argument("--sort", type=int, default=-1, help="band-sorted bundle order 0/1 (default: context's)")
     ap.add_argument("--ref-seconds", dest="ref_seconds", type=float, default=12.0)
     ap.add_argument("--traffic", type=float, default=None)
     ap.add_argument("--photmax", type=int, default=0, help="override bundles per cell (profiling runs)")

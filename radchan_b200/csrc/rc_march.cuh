@@ -99,6 +99,9 @@ __global__ void __launch_bounds__(256, MINB) k_march(MarchArgs a) {
     unsigned long long chunk_next = 0, chunk_end = 0;
     const unsigned long long total = (unsigned long long)a.total_tiles;
     const unsigned long long all_warps = (unsigned long long)gridDim.x * nwarps;
+    // lanes tracing a ray, and lanes whose ray belongs to buffer 1
+    // (warp-uniform; kept in step with the lanes' own flags)
+    unsigned amask = 0u, p1mask = 0u;
     // lane state
     bool active = false;
     int myb = 0, mypar = 0;
@@ -211,17 +214,17 @@ __global__ void __launch_bounds__(256, MINB) k_march(MarchArgs a) {
         }
         // ---- idle lanes take emitted bundles
         {
-            const bool need = !active;
-            const unsigned m = __ballot_sync(0xffffffffu, need);
+            const unsigned m = ~amask;
             const int navail = min(count, __popc(m));
-            bool fin = false;
-            if (need) {
+            bool took = false, fin = false;
+            if (!active) {
                 const int rank = __popc(m & lt);
                 if (rank < navail) {
                     const Emitted<R> &e = ws->ring[(head + rank) & (kRing - 1)];
                     place_bundle(r, S, e);
                     myb = e.b & 0xffff;
                     mypar = e.b >> 16;
+                    took = true;
                     active = level_advance(r, S);
                     if (!active) {
                         slots0[mypar * pool_max + myb] = r.De;
@@ -231,10 +234,15 @@ __global__ void __launch_bounds__(256, MINB) k_march(MarchArgs a) {
             }
             head = (head + navail) & (kRing - 1);
             count -= navail;
-            const unsigned f1 = __ballot_sync(0xffffffffu, fin && mypar == 1);
-            const unsigned f0 = __ballot_sync(0xffffffffu, fin && mypar == 0);
-            out0 -= __popc(f0);
-            out1 -= __popc(f1);
+            if (navail > 0) {
+                const unsigned tk = __ballot_sync(0xffffffffu, took);
+                const unsigned t1 = __ballot_sync(0xffffffffu, took && mypar == 1);
+                const unsigned fi = __ballot_sync(0xffffffffu, fin);
+                p1mask = (p1mask & ~tk) | t1;
+                amask = (amask | tk) & ~fi;
+                out1 -= __popc(fi & t1);
+                out0 -= __popc(fi & ~t1);
+            }
             __syncwarp();
         }
         // ---- step every active ray; stay in this loop until enough lanes
@@ -259,11 +267,12 @@ __global__ void __launch_bounds__(256, MINB) k_march(MarchArgs a) {
                 }
                 const unsigned fm = __ballot_sync(0xffffffffu, fin);
                 if (fm) {
-                    const int n1 = __popc(__ballot_sync(0xffffffffu, fin && mypar == 1));
+                    const int n1 = __popc(fm & p1mask);
                     out1 -= n1;
                     out0 -= __popc(fm) - n1;
+                    amask &= ~fm;
                 }
-                const int nidle = __popc(__ballot_sync(0xffffffffu, !active));
+                const int nidle = kWarp - __popc(amask);
                 if (nidle == kWarp) break;
                 if (nidle >= kFeedIdle && can_feed) break;
                 if (fm && ((((busy & emitted) & 1u) && out0 == 0) || (((busy & emitted) & 2u) && out1 == 0))) break;
