@@ -11,7 +11,9 @@ Recipe (nothing from the reference is copied into this repository):
        of a global array (read_tables.cpp:169-170); the patch writes
        probg[i][j][g] so no host memory outside the array is overwritten;
   3. rewrite the #define values of param.h (and the maxi/maxj/maxk initialisers)
-     for the configuration;
+     for the configuration; for the narrow-band configurations also nT/nQ/nB
+     in NarrowBand.h and the constant g-CDF probq (mc_gpu_noint.cu:34-36,
+     written for nQ = 16) as cumsum(wq) of the table set;
   4. compile with nvcc for sm_100a with the reference's own flags
      (--use_fast_math -ftz=true -prec-div=false, Makefile:20-24) together with
      oracle/ref_driver.cu into oracle/_ref/libref_<config>.so.
@@ -52,6 +54,22 @@ CONFIGS = {
                    levels=["imax"], levels_j=["jmax"], levels_k=["kmax"]),
 }
 
+# Narrow-band channel, 64^3 (100 bands x 8 g points x 64 temperatures of the
+# seeded synthetic tables), 3 levels 64/32/16 with maxs 5/5/1e5, photmax 256,
+# nVar 4, wall-flux kernel with an adiabatic west wall; "nb64" with the
+# band-sorted mode (srt = 1) as configured, "nb64s0" without it (its
+# replicates are independent, so its sigma is a fair parity reference).
+_NB = dict(num_gpu="1", p_col="1", imax="64", jmax="64", kmax="64", Lx="2.f", Ly="6.283185307179586f",
+           Lz="3.141592653589793f", fact_mesh="1.5", nVar="4", photmax="256", chanHeight="1.0", grid_num="3",
+           num_streams="2", blockdim="128", nblocks="4096", srt="1", grey="0", calcwalls="1", random="0",
+           floatpoint="0", epsw="1.f", epse="1.f", epss="1.f", epsn="1.f", epsb="1.f", epst="1.f", Tww="955",
+           Twe="573", Tws="0", Twn="0", Twb="0", Twt="0", adiabw="1", adiabe="0", toll="1.0e-3", tollS="1.0e-3",
+           bdw="2", bde="2", bds="1", bdn="1", bdb="1", bdt="1")
+for _name, _srt in (("nb64", "1"), ("nb64s0", "0")):
+    CONFIGS[_name] = dict(defines=dict(_NB, srt=_srt), levels=["imax", "imax/2", "imax/4"],
+                          levels_j=["jmax", "jmax/2", "jmax/4"], levels_k=["kmax", "kmax/2", "kmax/4"],
+                          narrowband=dict(nT="64", nQ="8", nB="100"))
+
 
 def _patch_mc(src: str) -> str:
     old_decl = "texture<myfloat, cudaTextureType2D, cudaReadModeElementType> tex_Ib;"
@@ -77,6 +95,33 @@ def _patch_tables(src: str) -> str:
     old = re.compile(r"probg\[nT\]\[nB\]\[nQ\] = g;(\s*)probg_h\[m\] = probg\[nT\]\[nB\]\[nQ\];")
     assert old.search(src)
     return old.sub(r"probg[i][j][g] = g;\1probg_h[m] = probg[i][j][g];", src)
+
+
+def _patch_probq(src: str, wq) -> str:
+    """The 16-entry probq initializer (mc_gpu_noint.cu:34-36) becomes
+    cumsum(wq) of the table set for other nQ."""
+    pat = re.compile(r"(__device__ __constant__ myfloat probq\[nQ\] = \{)[^}]*(\};)", re.S)
+    assert pat.search(src)
+    c, vals = 0.0, []
+    for w in wq:
+        c += float(w)
+        vals.append("%.9g" % c)
+    vals[-1] = "1.0"
+    return pat.sub(lambda m: m.group(1) + ",".join(vals) + m.group(2), src, count=1)
+
+
+def _patch_narrowband(src: str, nb: dict) -> str:
+    for k, v in nb.items():
+        pat = re.compile(r"^(#define\s+%s\s+)(\S+)" % re.escape(k), re.M)
+        assert pat.search(src), k
+        src = pat.sub(lambda m: m.group(1) + v, src, count=1)
+    return src
+
+
+def _table_wq():
+    sys.path.insert(0, ROOT)
+    from radchan_b200 import workloads as W
+    return list(W.tables_nb().arrays()["wq"])
 
 
 def _patch_param(src: str, cfg: dict) -> str:
@@ -105,9 +150,14 @@ def build(name: str, verbose: bool = False) -> str:
             shutil.copy(os.path.join(REF, "src", "montecarlo", f), mc)
         for f in PARAM_FILES:
             shutil.copy(os.path.join(REF, "src", "param", f), pa)
-        for path, fn in ((os.path.join(mc, "mc_gpu_noint.cu"), _patch_mc),
-                         (os.path.join(mc, "read_tables.cpp"), _patch_tables),
-                         (os.path.join(pa, "param.h"), lambda t: _patch_param(t, cfg))):
+        patches = [(os.path.join(mc, "mc_gpu_noint.cu"), _patch_mc),
+                   (os.path.join(mc, "read_tables.cpp"), _patch_tables),
+                   (os.path.join(pa, "param.h"), lambda t: _patch_param(t, cfg))]
+        if "narrowband" in cfg:
+            wq = _table_wq()
+            patches.append((os.path.join(mc, "mc_gpu_noint.cu"), lambda t: _patch_probq(t, wq)))
+            patches.append((os.path.join(pa, "NarrowBand.h"), lambda t: _patch_narrowband(t, cfg["narrowband"])))
+        for path, fn in patches:
             with open(path) as f:
                 text = f.read()
             with open(path, "w") as f:
