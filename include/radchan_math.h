@@ -128,10 +128,10 @@ RC_HD float rc_exp2i_f(int n) {
     return rc_u32_as_f32((uint32_t)(n + 127) << 23);
 }
 
-/* e^r - 1 for |r| <= ~0.35: r * (1 + r/2! + r^2/3! + ... + r^7/8!) */
+/* e^r - 1 for |r| <= ~0.35: r * (1 + r/2! + r^2/3! + ... + r^6/7!); the
+ * first omitted term, r^8/8!, is below 1.5e-8 relative (0.13 ulp). */
 RC_HD float rc_expm1_poly_f(float r) {
-    float p = 2.4801587642286904e-05f;          /* 1/8! */
-    p = fmaf(p, r, 1.9841270113829523e-04f);    /* 1/7! */
+    float p = 1.9841270113829523e-04f;          /* 1/7! */
     p = fmaf(p, r, 1.3888889225199819e-03f);    /* 1/6! */
     p = fmaf(p, r, 8.3333337679505348e-03f);    /* 1/5! */
     p = fmaf(p, r, 4.1666667908430099e-02f);    /* 1/4! */
@@ -148,7 +148,7 @@ RC_HD float rc_expf(float x) {
     if (x < -87.0f) return 0.0f;
     if (x > 88.0f) return rc_u32_as_f32(0x7f800000u);
     float n = rintf(x * RC_LOG2E_F);
-    float r = (x - n * RC_LN2_HI_F) - n * RC_LN2_LO_F;
+    float r = fmaf(-n, RC_LN2_LO_F, fmaf(-n, RC_LN2_HI_F, x));
     float p = rc_expm1_poly_f(r) + 1.0f;
     return p * rc_exp2i_f((int)n);
 }
@@ -160,7 +160,8 @@ RC_HD float rc_expf(float x) {
 RC_HD float rc_expm1f(float x) {
     x = fminf(fmaxf(x, -87.0f), 88.0f);
     float n = rintf(x * RC_LOG2E_F);
-    float r = (x - n * RC_LN2_HI_F) - n * RC_LN2_LO_F;
+    /* n * ln2_hi is exact, so the inner fma is the exact x - n ln2_hi */
+    float r = fmaf(-n, RC_LN2_LO_F, fmaf(-n, RC_LN2_HI_F, x));
     float p = rc_expm1_poly_f(r);
     float s = rc_exp2i_f((int)n);
     return fmaf(s, p, s - 1.0f);

@@ -48,9 +48,8 @@ template <typename R>
 struct DLevel {
     int im, jm, km, maxs;
     int rx, ry, rz;           // ratio to the next (coarser) level
-    int nbi, nbj;             // 4x4x4 bricks per x and y row of the coordinate array
     const R *xu, *yu, *zu;    // faces
-    const uint16_t *P;        // table coordinate of every cell, 4x4x4 bricks (see cell_index)
+    const uint16_t *P;        // table coordinate of every cell, i fastest (see cell_index)
     const uint16_t *Pw[6];    // wall emission temperature coordinates (or null)
 };
 
@@ -172,10 +171,11 @@ __device__ __forceinline__ R coord_frac(int q) {
     return (R)(q & 255) * (R)0.00390625;
 }
 
-// Offset of cell (i,j,k) (1-based) in a 4x4x4-brick array.
-__device__ __forceinline__ int cell_index(int i, int j, int k, int nbi, int nbj) {
-    const int a = i - 1, b = j - 1, c = k - 1;
-    return (((c >> 2) * nbj + (b >> 2)) * nbi + (a >> 2)) * 64 + ((a & 3) | ((b & 3) << 2) | ((c & 3) << 4));
+// Offset of cell (i,j,k) (1-based) in an im x jm x km array, i fastest.
+// (A 4x4x4-brick layout was measured 2-3% slower: its index arithmetic
+// costs more issue slots than its locality saves in L1 misses.)
+__device__ __forceinline__ int cell_index(int i, int j, int k, int im, int jm) {
+    return (i - 1) + im * ((j - 1) + jm * (k - 1));
 }
 
 // Linear interpolation in temperature along one table column at a clamped
@@ -288,7 +288,7 @@ __device__ __forceinline__ bool emit_bundle(Emitted<R> &e, const DSolve<R> &S, i
         nb = guided_index(S.cdf_f, S.guide_f, S.nB, u_b);
         g = (S.nQ > 1) ? bisect(S.probg + ((size_t)S.row * S.nB + nb) * S.nQ, S.nQ, u_g) : 0;
         const DLevel<R> &L0 = S.lev[0];
-        Pi = L0.P[cell_index(i, j, k, L0.nbi, L0.nbj)];
+        Pi = L0.P[cell_index(i, j, k, L0.im, L0.jm)];
         e.xp = S.xc[i];
     } else {
         // Lambertian: theta = acos(1 - 2u)/2 (+pi/2 on the east wall)
@@ -441,7 +441,7 @@ __device__ __forceinline__ void march_step(Ray<R> &r, const DSolve<R> &S, const 
     const R fxu = L.xu[r.ic - r.fx];
     const R fyu = L.yu[r.jc - r.fy];
     const R fzu = L.zu[r.kc - r.fz];
-    const int q = __ldg(&L.P[cell_index(r.ic, r.jc, r.kc, L.nbi, L.nbj)]);
+    const int q = __ldg(&L.P[cell_index(r.ic, r.jc, r.kc, L.im, L.jm)]);
     const KIRow<R> row = load_row(r.kicol + (q >> 8));
     const R dsx = (fxu - r.xp) * r.isx;
     const R dsy = (fyu - r.yp) * r.isy;

@@ -332,8 +332,6 @@ struct Impl : ImplBase {
                 LevelJob &jb = J.job[J.njobs++];
                 jb.dst = dst;
                 jb.type = type;
-                jb.nbi = (p.maxi[l] + 3) / 4;
-                jb.nbj = (p.maxj[l] + 3) / 4;
                 jb.im = p.maxi[l];
                 jb.jm = p.maxj[l];
                 jb.km = p.maxk[l];
@@ -347,9 +345,8 @@ struct Impl : ImplBase {
             };
             for (int l = 0; l < nl; ++l) {
                 const long long n = (long long)p.maxi[l] * p.maxj[l] * p.maxk[l];
-                const long long nbr = (long long)((p.maxi[l] + 3) / 4) * ((p.maxj[l] + 3) / 4) * ((p.maxk[l] + 3) / 4);
-                RC_CK(cudaMalloc((void **)&s.d_levT[l], nbr * 64 * sizeof(uint16_t)));
-                RC_CK(cudaMemset(s.d_levT[l], 0, nbr * 64 * sizeof(uint16_t)));
+                RC_CK(cudaMalloc((void **)&s.d_levT[l], n * sizeof(uint16_t)));
+                RC_CK(cudaMemset(s.d_levT[l], 0, n * sizeof(uint16_t)));
                 add_job(s.d_levT[l], 0, l, 0, n);
                 for (int w = 0; w < 6; ++w) {
                     const int t = c->wt[w];
@@ -554,8 +551,6 @@ struct Impl : ImplBase {
             L.yu = d_yu[l];
             L.zu = d_zu[l];
             L.P = s.d_levT[l];
-            L.nbi = (L.im + 3) / 4;
-            L.nbj = (L.jm + 3) / 4;
             for (int w = 0; w < 6; ++w) L.Pw[w] = s.d_lw[l][w];
         }
         d.imax = p.imax;

@@ -235,8 +235,7 @@ __device__ __forceinline__ float tex_sample(const float *T, int nx, int ny, int 
 // or the emission temperature of a wall at that level (:392-396, 468-472).
 struct LevelJob {
     void *dst;
-    int type;     // 0 cells (4x4x4 bricks), 1 + w: wall w (linear)
-    int nbi, nbj; // bricks per x / y row (cells)
+    int type;     // 0 cells, 1 + w: wall w
     int im, jm, km;
     int rx, ry, rz;   // fine cells per level cell (imax/im ...)
     int face;     // wall sampled at the face (1) or at the first cell (0)
@@ -270,7 +269,7 @@ __global__ void k_levels(const float *__restrict__ T, int imax, int jmax, int km
             const float t1 = ((float)ic - 0.5f) * rxf + 1.0f;
             const float t2 = ((float)jc - 0.5f) * ryf + 1.0f;
             const float t3 = ((float)kc - 0.5f) * rzf + 1.0f;
-            dst[cell_index(ic, jc, kc, J.nbi, J.nbj)] =
+            dst[cell_index(ic, jc, kc, J.im, J.jm)] =
                 (uint16_t)table_coord((R)tex_sample(T, nx, ny, nz, t1, t2, t3), T0, inv_dT, nT);
         } else {
             const int w = J.type - 1;

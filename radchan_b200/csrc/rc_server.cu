@@ -153,8 +153,7 @@ size_t context_bytes(const rc_params &p, int photmax) {
     const double ncf = (double)p.imax * p.jmax * kl, nwc = 2.0 * p.jmax * kl;
     double slot = nfield * 4 + ncf * 24 + nwc * 24 + 2.0 * p.jmax * p.kmax * 2;
     for (int l = 0; l < p.grid_num; ++l) {
-        const double nbr = (double)((p.maxi[l] + 3) / 4) * ((p.maxj[l] + 3) / 4) * ((p.maxk[l] + 3) / 4);
-        slot += nbr * 64 * 2 + 2.0 * ((double)p.maxj[l] * p.maxk[l] + (double)p.maxi[l] * p.maxk[l] +
+        slot += (double)p.maxi[l] * p.maxj[l] * p.maxk[l] * 2 + 2.0 * ((double)p.maxj[l] * p.maxk[l] + (double)p.maxi[l] * p.maxk[l] +
                                       (double)p.maxi[l] * p.maxj[l]) * 2;
     }
     const int nB = p.grey ? p.grey_nB : p.nB, nT = p.grey ? p.grey_nT : p.nT, nQ = p.grey ? 1 : p.nQ;
