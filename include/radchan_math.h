@@ -115,6 +115,15 @@ RC_HD float rc_u01(uint32_t x) {
 }
 
 /* ------------------------------------------------------------------ */
+/* table interpolation                                                 */
+/* ------------------------------------------------------------------ */
+/* a0 (1 - w) + a1 w, the product a0 (1 - w) rounded and a1 w added in one
+ * fused multiply-add (one rounding fewer than the plain expression, and
+ * one instruction fewer on the device). */
+RC_HD float rc_lerpf(float a0, float a1, float w) { return fmaf(a1, w, a0 * (1.0f - w)); }
+RC_HD double rc_lerp(double a0, double a1, double w) { return fma(a1, w, a0 * (1.0 - w)); }
+
+/* ------------------------------------------------------------------ */
 /* exp / expm1, single precision                                       */
 /* ------------------------------------------------------------------ */
 /* ln2 = RC_LN2_HI_F + RC_LN2_LO_F; the high part keeps 16 significant bits

@@ -30,11 +30,15 @@ template <> struct M<float> {
     static float expm1_(float x) { return rc_expm1f(x); }
     static float sqrt_(float x) { return sqrtf(x); }
     static void sincos2pi_(float u, float *s, float *c) { rc_sincos2pif(u, s, c); }
+    static float fma_(float a, float b, float c) { return fmaf(a, b, c); }
+    static float lerp_(float a0, float a1, float w) { return rc_lerpf(a0, a1, w); }
 };
 template <> struct M<double> {
     static double expm1_(double x) { return rc_expm1(x); }
     static double sqrt_(double x) { return sqrt(x); }
     static void sincos2pi_(double u, double *s, double *c) { rc_sincos2pi(u, s, c); }
+    static double fma_(double a, double b, double c) { return fma(a, b, c); }
+    static double lerp_(double a0, double a1, double w) { return rc_lerp(a0, a1, w); }
 };
 
 // ---------------------------------------------------------------- grid
@@ -119,7 +123,7 @@ R lerpq(const R *col, int nT, int q) {
     int i0 = q >> 8;
     int i1 = std::min(i0 + 1, nT - 1);
     R a = (R)(q & 255) * (R)0.00390625;
-    return col[i0] * ((R)1 - a) + col[i1] * a;
+    return M<R>::lerp_(col[i0], col[i1], a);
 }
 
 template <typename R>
@@ -388,7 +392,7 @@ struct Problem {
     }
 
     void deposit(Beam &ray, double &De, R Ibmax, R ratioI, R invTi4, R e) const {
-        R c = (Ibmax * ray.tra) * (invTi4 * e - (R)1);
+        R c = (Ibmax * ray.tra) * M<R>::fma_(invTi4, e, (R)-1);
         c = c * ratioI;
         De -= (double)c;
         ray.tra = 0;
@@ -473,20 +477,20 @@ struct Problem {
             if (ds > dsy) ds = dsy;
             if (ds > dsz) ds = dsz;
             if (ds == dsx) ray.xp = fxu;
-            else ray.xp = ray.xp + ds * ray.sx;
+            else ray.xp = M<R>::fma_(ds, ray.sx, ray.xp);
             if (ds == dsy) ray.yp = fyu;
-            else ray.yp = ray.yp + ds * ray.sy;
+            else ray.yp = M<R>::fma_(ds, ray.sy, ray.yp);
             if (ds == dsz) ray.zp = fzu;
-            else ray.zp = ray.zp + ds * ray.sz;
+            else ray.zp = M<R>::fma_(ds, ray.sz, ray.zp);
             R em = M<R>::expm1_(-(ds * absco));
             R alpha = -em;
-            R dI = invTi4 * blackpow - (R)1;
+            R dI = M<R>::fma_(invTi4, blackpow, (R)-1);
             R c = Ibmax * ray.tra;
             c = c * alpha;
             c = c * ratioI;
             c = c * dI;
             De -= (double)c;
-            ray.tra = ray.tra * ((R)1 + em);
+            ray.tra = M<R>::fma_(ray.tra, em, ray.tra);
             if (ray.tra < tol) {
                 R c2 = (Ibmax * ray.tra) * ratioI;
                 c2 = c2 * dI;

@@ -11,17 +11,18 @@
 // Arithmetic contract (shared with the CPU oracle, which restates the same
 // operations in the same order so that sampled bands, g points, visited
 // cells and per-bundle tallies agree bit for bit):
-//   * no FMA contraction (nvcc -fmad=false); explicit fmaf() only inside
-//     radchan_math.h;
+//   * no automatic FMA contraction (nvcc -fmad=false, g++ -ffp-contract=off);
+//     every fused multiply-add is written out (fma_ here, the same call in
+//     the oracle, fmaf() in radchan_math.h), so both sides round alike;
 //   * face distance ds = (face - p) * (1/s), the reciprocal formed once per
-//     direction change;
+//     direction change; positions p = fma(ds, s, p) on the axes not crossed;
 //   * table coordinate q = rint(256 * clamp((T - T0) * (1/dT), 0, nT-1)),
 //     8 fractional bits (the weight precision of the texture unit the
 //     reference interpolates with), stored as uint16 per cell of every
-//     multigrid level; v = col[i0]*(1-a) + col[i1]*a with i0 = q >> 8,
-//     i1 = min(i0 + 1, nT - 1), a = (q & 255) / 256;
-//   * alpha = -expm1(-(ds*k)), tra *= (1 + expm1(-(ds*k)));
-//   * step tally c = (((Ibmax*tra)*alpha)*ratioI)*(invTi4*Ib - 1) in the
+//     multigrid level; v = fma(col[i1], a, col[i0]*(1-a)) (rc_lerpf) with
+//     i0 = q >> 8, i1 = min(i0 + 1, nT - 1), a = (q & 255) / 256;
+//   * em = expm1(-(ds*k)), alpha = -em, tra = fma(tra, em, tra);
+//   * step tally c = (((Ibmax*tra)*alpha)*ratioI)*fma(invTi4, Ib, -1) in the
 //     march precision, accumulated into an FP64 bundle sum;
 //   * per-bundle sums are added in bundle order within a chunk of
 //     rays_per_thread bundles, chunk sums in chunk order, and replicate
@@ -121,6 +122,8 @@ template <typename R> struct RT;
 template <> struct RT<float> {
     static __device__ __forceinline__ float expm1_(float x) { return rc_expm1f(x); }
     static __device__ __forceinline__ float sqrt_(float x) { return sqrtf(x); }
+    static __device__ __forceinline__ float fma_(float a, float b, float c) { return fmaf(a, b, c); }
+    static __device__ __forceinline__ float lerp_(float a0, float a1, float w) { return rc_lerpf(a0, a1, w); }
     static __device__ __forceinline__ void sincos2pi_(float u, float *s, float *c) { rc_sincos2pif(u, s, c); }
     static __device__ __forceinline__ float fmin_(float a, float b) { return fminf(a, b); }
     static __device__ __forceinline__ float fmax_(float a, float b) { return fmaxf(a, b); }
@@ -129,6 +132,8 @@ template <> struct RT<float> {
 template <> struct RT<double> {
     static __device__ __forceinline__ double expm1_(double x) { return rc_expm1(x); }
     static __device__ __forceinline__ double sqrt_(double x) { return sqrt(x); }
+    static __device__ __forceinline__ double fma_(double a, double b, double c) { return fma(a, b, c); }
+    static __device__ __forceinline__ double lerp_(double a0, double a1, double w) { return rc_lerp(a0, a1, w); }
     static __device__ __forceinline__ void sincos2pi_(double u, double *s, double *c) { rc_sincos2pi(u, s, c); }
     static __device__ __forceinline__ double fmin_(double a, double b) { return fmin(a, b); }
     static __device__ __forceinline__ double fmax_(double a, double b) { return fmax(a, b); }
@@ -183,7 +188,7 @@ __device__ __forceinline__ int cell_index(int i, int j, int k, int im, int jm) {
 // mc_gpu_noint.cu:341-345, memory_copy_noint.cu:241-245).
 template <typename R>
 __device__ __forceinline__ R lerp_at(const R *col, int i0, int i1, R a) {
-    return col[i0] * ((R)1 - a) + col[i1] * a;
+    return RT<R>::lerp_(col[i0], col[i1], a);
 }
 template <typename R>
 __device__ __forceinline__ R tab_lerp(const R *col, int nT, int q) {
@@ -337,11 +342,11 @@ __device__ __forceinline__ bool emit_bundle(Emitted<R> &e, const DSolve<R> &S, i
     // OERM weights
     const KIRow<R> row = S.ki[((size_t)nb * S.nQ + g) * S.nT + (Pi >> 8)];
     const R fr = coord_frac<R>(Pi);
-    const R Ib_i = row.ib0 * ((R)1 - fr) + row.ib1 * fr;
+    const R Ib_i = RT<R>::lerp_(row.ib0, row.ib1, fr);
     if (!(Ib_i > (R)0)) return false;
     e.invTi4 = (R)1 / Ib_i;
     if (kind == 0) {
-        const R k_i = row.k0 * ((R)1 - fr) + row.k1 * fr;
+        const R k_i = RT<R>::lerp_(row.k0, row.k1, fr);
         const R den = S.den_f[(size_t)nb * S.nQ + g];
         if (!(den > (R)0)) return false;
         e.ratioI = (Ib_i * k_i) / den;
@@ -389,7 +394,7 @@ __device__ __forceinline__ void place_bundle(Ray<R> &r, const DSolve<R> &S, cons
 // (:398-399 and its siblings): De -= Ibmax*tra*(invTi4*e - 1)*ratioI.
 template <typename R>
 __device__ __forceinline__ void wall_deposit(Ray<R> &r, R e) {
-    R c = (r.Ibmax * r.tra) * (r.invTi4 * e - (R)1);
+    R c = (r.Ibmax * r.tra) * RT<R>::fma_(r.invTi4, e, (R)-1);
     c = c * r.ratioI;
     r.De -= (double)c;
     r.tra = (R)0;
@@ -419,7 +424,7 @@ __device__ __forceinline__ void hit_wall(Ray<R> &r, const DSolve<R> &S, const DL
         const int q = L.Pw[w][idx];
         const KIRow<R> row = r.kicol[q >> 8];
         const R fr = coord_frac<R>(q);
-        wall_deposit(r, row.ib0 * ((R)1 - fr) + row.ib1 * fr);
+        wall_deposit(r, RT<R>::lerp_(row.ib0, row.ib1, fr));
     } else if (t == 3) {  // specular
         switch (w) {
             case RC_WEST: r.xp = (R)0; r.sx = -r.sx; r.isx = -r.isx; r.ic = 1; r.fx = r.sx < (R)0; break;
@@ -447,23 +452,23 @@ __device__ __forceinline__ void march_step(Ray<R> &r, const DSolve<R> &S, const 
     const R dsy = (fyu - r.yp) * r.isy;
     const R dsz = (fzu - r.zp) * r.isz;
     const R a = coord_frac<R>(q);
-    const R absco = row.k0 * ((R)1 - a) + row.k1 * a;
-    const R blackpow = row.ib0 * ((R)1 - a) + row.ib1 * a;
+    const R absco = RT<R>::lerp_(row.k0, row.k1, a);
+    const R blackpow = RT<R>::lerp_(row.ib0, row.ib1, a);
     R ds = dsx;
     if (ds > dsy) ds = dsy;
     if (ds > dsz) ds = dsz;
-    r.xp = (ds == dsx) ? fxu : r.xp + ds * r.sx;
-    r.yp = (ds == dsy) ? fyu : r.yp + ds * r.sy;
-    r.zp = (ds == dsz) ? fzu : r.zp + ds * r.sz;
+    r.xp = (ds == dsx) ? fxu : RT<R>::fma_(ds, r.sx, r.xp);
+    r.yp = (ds == dsy) ? fyu : RT<R>::fma_(ds, r.sy, r.yp);
+    r.zp = (ds == dsz) ? fzu : RT<R>::fma_(ds, r.sz, r.zp);
     const R em = RT<R>::expm1_(-(ds * absco));
     const R alpha = -em;
-    const R dI = r.invTi4 * blackpow - (R)1;
+    const R dI = RT<R>::fma_(r.invTi4, blackpow, (R)-1);
     R c = r.Ibmax * r.tra;
     c = c * alpha;
     c = c * r.ratioI;
     c = c * dI;
     r.De -= (double)c;
-    r.tra = r.tra * ((R)1 + em);
+    r.tra = RT<R>::fma_(r.tra, em, r.tra);
     if (r.tra < r.tol) {  // cutoff: deposit the rest here (:365-370)
         R c2 = (r.Ibmax * r.tra) * r.ratioI;
         c2 = c2 * dI;
