@@ -19,7 +19,8 @@ Legs on one GPU (skipped with --no-legs):
   batched  64 uneven problems (grids 16..96 per axis, half grey, half
          narrow-band 20-100 bands, photmax 32/128/512): plain one solve per
          launch vs one persistent launch from a CUDA graph vs the
-         continuous-batching server, solves/s by wall clock.
+         continuous-batching server, solves/s by wall clock;
+  batched_small  the same with edges 16..32 and photmax 32/128.
 
 --serve runs the open-loop serving benchmark instead (Poisson arrivals at
 --load x measured capacity, tolerance-driven photmax, p50/p99 latency);
@@ -236,13 +237,13 @@ def leg_at_tolerance(p, tabs, T, rel0, dev, flush, tol=0.01, steps=2):
             "solves_per_s": steps / sec, "bundles_per_s": bundles / sec, "steps": steps}
 
 
-def batch_setup(dev, n=64):
+def batch_setup(dev, n=64, edges=(16, 24, 32, 48, 64, 96), photmaxes=(32, 128, 512)):
     """The uneven-problem mix: 64 problems, grid edges from
     {16,24,32,48,64,96} per axis, half grey and half narrow-band (20-100
     bands x 8 g), photmax from {32,128,512}; seeded fields and tables."""
     from radchan_b200 import api
     from radchan_b200 import workloads as W
-    probs = W.batch_problems(n=n)
+    probs = W.batch_problems(n=n, edges=edges, photmaxes=photmaxes)
     items = []
     for pr in probs:
         p = pr["params"]
@@ -255,13 +256,13 @@ def batch_setup(dev, n=64):
     return items
 
 
-def leg_batched(dev, passes=2):
+def leg_batched(dev, passes=2, **mix):
     """Plain (one solve per launch, host arrays in and out, one after the
     other) vs batched (every solve in one persistent launch replayed from a
     CUDA graph) vs served (all submitted to the continuous-batching server at
     once) on the uneven mix.  Wall clock per pass of all 64 solves."""
     from radchan_b200 import api
-    items = batch_setup(dev)
+    items = batch_setup(dev, **mix)
     work = [it["p"].imax * it["p"].jmax * it["p"].kmax * it["p"].nVar * it["p"].photmax for it in items]
     big = items[int(np.argmax(work))]
     knobs = big["s"].autotune(big["T"], pilot_photmax=min(big["p"].photmax, 128))
@@ -537,6 +538,9 @@ def run_ours(args, ws, rank, local):
     if ws == 1 and not args.no_legs:
         line["at_1pct"] = leg_at_tolerance(p, tabs, T, rel_std, dev, flush)
         line["batched"] = leg_batched(dev)
+        # the same recipe restricted to small problems (edges 16-32, photmax
+        # 32/128), where one solve does not fill the GPU
+        line["batched_small"] = leg_batched(dev, edges=(16, 24, 32), photmaxes=(32, 128))
     if rank == 0 and not args.no_cpu_baseline:
         cb = cpu_sample(p, tabs, T, seconds=args.ref_seconds)
         line["cpu_baseline"] = {"value": cb["bundles"] / cb["seconds"], "unit": "bundles/s",
