@@ -49,6 +49,7 @@ template <typename R>
 struct DLevel {
     int im, jm, km, maxs;
     int rx, ry, rz;           // ratio to the next (coarser) level
+    unsigned mrx, mry, mrz;   // floor(2^32 / r) + 1 (0 for r = 1): (n + r - 1) / r as a multiply-high
     const R *xu, *yu, *zu;    // faces
     const uint16_t *P;        // table coordinate of every cell, i fastest (see cell_index)
     const uint16_t *Pw[6];    // wall emission temperature coordinates (or null)
@@ -497,6 +498,14 @@ __device__ __forceinline__ void march_step(Ray<R> &r, const DSolve<R> &S, const 
     r.counter += 1;
 }
 
+// Index of the coarse cell holding fine cell n (1-based): (n + r - 1) / r,
+// as floor(n' m / 2^32) with m = floor(2^32 / r) + 1, exact for n' r < 2^32
+// (the host checks it); m = 0 stands for r = 1.
+__device__ __forceinline__ int coarse_index(int n, int r, unsigned m) {
+    const unsigned np = (unsigned)(n + r - 1);
+    return (int)(m ? __umulhi(np, m) : np);
+}
+
 // Advance to coarser levels while the step budget of the current level is
 // spent (:210-224).  Returns false when the ray must stop (budget of the
 // last level spent).
@@ -505,9 +514,9 @@ __device__ __forceinline__ bool level_advance(Ray<R> &r, const DSolve<R> &S) {
     while (r.counter >= S.lev[r.lev].maxs) {
         if (r.lev >= S.nlev - 1) return false;
         const DLevel<R> &L = S.lev[r.lev];
-        r.ic = (r.ic + L.rx - 1) / L.rx;
-        r.jc = (r.jc + L.ry - 1) / L.ry;
-        r.kc = (r.kc + L.rz - 1) / L.rz;
+        r.ic = coarse_index(r.ic, L.rx, L.mrx);
+        r.jc = coarse_index(r.jc, L.ry, L.mry);
+        r.kc = coarse_index(r.kc, L.rz, L.mrz);
         r.lev += 1;
         r.counter = 0;
     }

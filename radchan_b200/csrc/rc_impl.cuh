@@ -547,6 +547,9 @@ struct Impl : ImplBase {
             } else {
                 L.rx = L.ry = L.rz = 1;
             }
+            L.mrx = magic32(L.rx);
+            L.mry = magic32(L.ry);
+            L.mrz = magic32(L.rz);
             L.xu = d_xu[l];
             L.yu = d_yu[l];
             L.zu = d_zu[l];
@@ -616,14 +619,22 @@ struct Impl : ImplBase {
     static unsigned long long magic(unsigned long long d) {
         return d <= 1 ? 0ull : (~0ull / d) + 1ull;
     }
+    static unsigned magic32(unsigned d) { return d <= 1 ? 0u : (unsigned)(0xffffffffu / d) + 1u; }
 
     // fdiv is exact when numerator * divisor < 2^64 at every division of the
     // item decomposition.
     bool decomposition_fits(const DSolve<R> &d) const {
         const long double lim = 18446744073709551615.0L;
         const long double n = (long double)d.n_items;
-        return n * d.nchunk < lim && n * d.nVar < lim && n * c->p.imax < lim && n * c->p.jmax < lim &&
-               n * (long double)d.nwc < lim;
+        bool ok = n * d.nchunk < lim && n * d.nVar < lim && n * c->p.imax < lim && n * c->p.jmax < lim &&
+                  n * (long double)d.nwc < lim;
+        // coarse_index is exact when (n + r - 1) * r < 2^32 on every axis
+        for (int l = 0; l + 1 < d.nlev; ++l) {
+            const DLevel<R> &L = d.lev[l];
+            ok = ok && (double)(L.im + L.rx) * L.rx < 4294967296.0 && (double)(L.jm + L.ry) * L.ry < 4294967296.0 &&
+                 (double)(L.km + L.rz) * L.rz < 4294967296.0;
+        }
+        return ok;
     }
 
     size_t partial_count(int rpt) const {
