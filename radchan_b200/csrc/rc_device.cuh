@@ -494,7 +494,27 @@ __device__ __forceinline__ void march_step(Ray<R> &r, const DSolve<R> &S, const 
         nidx = r.kc;
         lim = L.km + 1;
     }
-    if (nidx == 0 || nidx == lim) hit_wall(r, S, L, 2 * axis + (nidx != 0));
+    if (nidx == 0 || nidx == lim) {
+        const int w = 2 * axis + (nidx != 0);
+        if (S.wtype[w] == 1) {
+            // periodic (the common wall of the channel): re-enter through the
+            // opposite face, on a short path of its own
+            const bool hi = nidx != 0;
+            const int ni = hi ? 1 : lim - 1;
+            if (axis == 0) {
+                r.ic = ni;
+                r.xp = hi ? (R)0 : S.Lx;
+            } else if (axis == 1) {
+                r.jc = ni;
+                r.yp = hi ? (R)0 : S.Ly;
+            } else {
+                r.kc = ni;
+                r.zp = hi ? (R)0 : S.Lz;
+            }
+        } else {
+            hit_wall(r, S, L, w);
+        }
+    }
     r.counter += 1;
 }
 
