@@ -478,22 +478,14 @@ __device__ __forceinline__ void march_step(Ray<R> &r, const DSolve<R> &S, const 
     }
     // crossed axis (ties: x only if strictly smallest, :375-377, 524)
     const int axis = (dsx < dsy) ? ((dsx < dsz) ? 0 : 2) : ((dsy < dsz) ? 1 : 2);
-    const int f = axis == 0 ? r.fx : (axis == 1 ? r.fy : r.fz);
+    const bool ax0 = axis == 0, ax1 = axis == 1;
+    const int f = ax0 ? r.fx : (ax1 ? r.fy : r.fz);
     const int dlt = f ? -1 : 1;
-    int nidx, lim;
-    if (axis == 0) {
-        r.ic += dlt;
-        nidx = r.ic;
-        lim = L.im + 1;
-    } else if (axis == 1) {
-        r.jc += dlt;
-        nidx = r.jc;
-        lim = L.jm + 1;
-    } else {
-        r.kc += dlt;
-        nidx = r.kc;
-        lim = L.km + 1;
-    }
+    r.ic += ax0 ? dlt : 0;
+    r.jc += ax1 ? dlt : 0;
+    r.kc += (axis == 2) ? dlt : 0;
+    const int nidx = ax0 ? r.ic : (ax1 ? r.jc : r.kc);
+    const int lim = (ax0 ? L.im : (ax1 ? L.jm : L.km)) + 1;
     if (nidx == 0 || nidx == lim) {
         const int w = 2 * axis + (nidx != 0);
         if (S.wtype[w] == 1) {
