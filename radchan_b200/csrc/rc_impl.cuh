@@ -7,7 +7,7 @@
 // uploaded once per context and stay resident; a solve copies only the
 // temperature field and runs
 //   k_init_scalars -> k_tmax -> k_setup1 -> [k_grey_ib] -> k_setup2 ->
-//   k_levels -> k_march -> k_tally
+//   k_levels -> k_patch_desc -> k_march -> k_tally_multi
 // on the context's stream without any host synchronisation.
 #include <cuda_runtime.h>
 #include <stdio.h>
@@ -54,9 +54,11 @@ struct TallyOut {
     float *Qc, *Sc, *Wq, *Ws;
 };
 
+// Replicate sums -> per-cell mean and variance of the mean
+// (kernel_fluid :229-239, kernel_surface :1468-1478), into compact FP64 and
+// FP32 outputs; one solve per blockIdx.y.
 template <typename R>
 __global__ void k_tally_multi(const DSolve<R> *solves, const TallyOut *outs) {
-    // one solve per blockIdx.y; reuse the single-solve body
     const int s = blockIdx.y;
     const TallyOut &o = outs[s];
     const DSolve<R> &S = solves[s];

@@ -296,57 +296,6 @@ __global__ void k_levels(const float *__restrict__ T, int imax, int jmax, int km
 }
 
 // ---------------------------------------------------------------------------
-// tally: replicate sums -> mean and variance (kernel_fluid :229-239,
-// kernel_surface :1468-1478), compact outputs
-// ---------------------------------------------------------------------------
-template <typename R>
-__global__ void k_tally(const DSolve<R> *Sp, double *q64, double *var64, double *qw64, double *vw64, float *Qc,
-                        float *Sc, float *Wq, float *Ws) {
-    const DSolve<R> &S = *Sp;
-    const long long ncf = (long long)S.imax * S.jmax * S.kloc;
-    const long long ncw = (long long)S.nwalls * S.jmax * S.kloc;
-    const int nVar = S.nVar, np = S.nparts;
-    double a = 0.0;
-    if (nVar > 1) {
-        a = 1. / (nVar - 0.5);
-        a = a * 1. / (nVar - 1);
-    }
-    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < ncf + ncw;
-         c += (long long)gridDim.x * blockDim.x) {
-        const double *p = S.partial + c * nVar * np;
-        double sum = 0.0;
-        for (int v = 0; v < nVar; ++v) {
-            double dv = 0.0;
-            for (int q = 0; q < np; ++q) dv += p[v * np + q];
-            sum += dv;
-        }
-        const double mean = sum / nVar;
-        double var = 0.0;
-        for (int v = 0; v < nVar; ++v) {
-            double dv = 0.0;
-            for (int q = 0; q < np; ++q) dv += p[v * np + q];
-            const double d = dv - mean;
-            var += a * d * d;
-        }
-        if (c < ncf) {
-            if (q64) q64[c] = mean;
-            if (var64) var64[c] = var;
-            Qc[c] = (float)mean;
-            Sc[c] = (float)sqrt(var);
-        } else {
-            const long long cw = c - ncf;
-            const long long nwc = (long long)S.jmax * S.kloc;
-            const int slot = (int)(cw / nwc);
-            const long long o = (long long)S.wall_id[slot] * nwc + (cw % nwc);
-            if (qw64) qw64[o] = mean;
-            if (vw64) vw64[o] = var;
-            Wq[o] = (float)mean;
-            Ws[o] = (float)sqrt(var);
-        }
-    }
-}
-
-// ---------------------------------------------------------------------------
 // bundle traces: one thread per requested bundle, same device functions
 // ---------------------------------------------------------------------------
 template <typename R>
