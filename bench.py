@@ -144,13 +144,22 @@ def dist_init():
 
 
 def allreduce_max(x, ws):
+    """Max of a per-rank timing over all ranks (the job is as slow as its
+    slowest replica); on the device for NCCL, on the host for gloo."""
     if ws == 1:
         return x
     import torch
     import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+def replica_value(units_per_rank, seconds, ws):
+    """Whole-job throughput of ws independent replicas: the units all ranks
+    processed over the slowest rank's time (max over ranks)."""
+    return units_per_rank * ws / allreduce_max(seconds, ws)
 
 
 def barrier(ws):
@@ -505,7 +514,7 @@ def run_ours(args, ws, rank, local):
     barrier(ws)
     t_dev = sum(ms_solve) / 1000.0
     t_max = allreduce_max(t_dev, ws)
-    value = bundles * ws / t_max
+    value = bundles * ws / t_max  # == replica_value(bundles, t_dev, ws)
     # e2e through the public API with host buffers
     Qh = np.zeros(api.result_shape(p), np.float32)
     Sh = np.zeros(api.result_shape(p), np.float32)

@@ -114,3 +114,28 @@ def test_submit_validation():
     with pytest.raises(L.RadChanError):
         srv.submit(pn, W.channel_field(pn), table_set=3)  # unknown table set
     srv.close()
+
+
+def test_request_arriving_during_a_long_solve_finishes_first():
+    """Continuous batching: a small request submitted while a long solve is
+    on the GPU joins the next quantum and completes long before it."""
+    import time
+    tabs = W.tables_nb(nB=40, nQ=4, nT=32)
+    big = W.channel_params(64, 64, 64, photmax=4096, nVar=4, nB=40, nQ=4, nT=32)
+    small = W.channel_params(16, 8, 8, photmax=16, nVar=4, nB=40, nQ=4, nT=32)
+    Tb, Ts = W.channel_field(big, seed=1), W.channel_field(small, seed=2)
+    srv = api.Server()
+    ts = srv.add_tables(tabs)
+    # warm the two problem classes (context creation is not what is measured)
+    srv.wait(srv.submit(small, Ts, table_set=ts))
+    q = api.copy_params(big)
+    q.photmax = 16
+    srv.wait(srv.submit(q, Tb, table_set=ts))
+    a = srv.submit(big, Tb, table_set=ts)
+    time.sleep(0.05)
+    b = srv.submit(small, Ts, table_set=ts)
+    rb, ra = srv.wait(b), srv.wait(a)
+    assert rb.t_done < ra.t_done
+    assert rb.t_submit > ra.t_admit          # it arrived while the long solve ran
+    assert rb.latency < 0.25 * ra.latency
+    srv.close()
