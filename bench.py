@@ -95,7 +95,7 @@ class ClockSampler:
         try:
             self.f = open(self.path, "w")
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.dev), "--query-gpu=" + self.FIELDS,
-                                          "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
+                                          "--format=csv,noheader,nounits", "-lms", "50"], stdout=self.f,
                                          stderr=subprocess.DEVNULL)
         except Exception:
             self.proc = None
@@ -550,7 +550,7 @@ def run_ours(args, ws, rank, local):
         # the same recipe restricted to small problems (edges 16-32, photmax
         # 32/128), where one solve does not fill the GPU
         line["batched_small"] = leg_batched(dev, edges=(16, 24, 32), photmaxes=(32, 128))
-    if rank == 0 and not args.no_cpu_baseline:
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         cb = cpu_sample(p, tabs, T, seconds=args.ref_seconds)
         line["cpu_baseline"] = {"value": cb["bundles"] / cb["seconds"], "unit": "bundles/s",
                                 "cores": os.cpu_count() or 1, "kind": "port",
