@@ -96,7 +96,7 @@ struct rc_server {
     long long quantum_tiles = kQuantumTiles;
     int policy = RC_SCHED_SRPT;
     long long quanta = 0;
-    std::vector<TableSet> tables;
+    std::vector<std::unique_ptr<TableSet>> tables;  // stable addresses: appended while the worker reads
     std::mutex mu;
     std::condition_variable cv_work, cv_done;
     std::deque<SrvReq *> queue;
@@ -245,7 +245,10 @@ int acquire_context(rc_server *sv, SrvReq *r) {
     const size_t need = context_bytes(r->p, std::max(r->photmax, kPilotPhotmax));
     for (size_t i = 0; i < sv->pool.size() && sv->hbm_in_use + need > sv->budget;) {
         if (!sv->pool[i].busy) {
-            sv->hbm_in_use -= sv->pool[i].bytes;
+            {
+                std::lock_guard<std::mutex> lk(sv->mu);
+                sv->hbm_in_use -= sv->pool[i].bytes;
+            }
             rc_destroy(sv->pool[i].ctx);
             sv->pool.erase(sv->pool.begin() + i);
         } else {
@@ -258,7 +261,12 @@ int acquire_context(rc_server *sv, SrvReq *r) {
     if (rc) return rc;
     if (!r->p.grey) {
         rc_tables v;
-        sv->tables[r->table_set].view(&v);
+        const TableSet *ts;
+        {
+            std::lock_guard<std::mutex> lk(sv->mu);
+            ts = sv->tables[r->table_set].get();
+        }
+        ts->view(&v);
         rc = rc_set_tables(c, &v);
         if (rc) {
             const std::string m = c->err;
@@ -267,6 +275,7 @@ int acquire_context(rc_server *sv, SrvReq *r) {
         }
     }
     sv->pool.push_back(PoolCtx{c, need, r->key, true});
+    std::lock_guard<std::mutex> lk(sv->mu);
     sv->hbm_in_use += need;
     r->ctx = c;
     return RC_OK;
@@ -294,6 +303,7 @@ void account_photmax(rc_server *sv, SrvReq *r) {
         if (pc.ctx == r->ctx) {
             const size_t b = context_bytes(r->p, r->photmax);
             if (b > pc.bytes) {
+                std::lock_guard<std::mutex> lk(sv->mu);
                 sv->hbm_in_use += (double)(b - pc.bytes);
                 pc.bytes = b;
             }
@@ -655,8 +665,8 @@ int rc_server_create(int device, double hbm_budget_bytes, int max_inflight, rc_s
 
 int rc_server_add_tables(rc_server *sv, const rc_tables *t, int *table_set) {
     if (!sv || !t || !table_set) return set_err(nullptr, RC_E_INVALID, "NULL argument");
-    TableSet ts;
-    ts.from_view(t);
+    auto ts = std::make_unique<TableSet>();
+    ts->from_view(t);
     std::lock_guard<std::mutex> lk(sv->mu);
     sv->tables.push_back(std::move(ts));
     *table_set = (int)sv->tables.size() - 1;
