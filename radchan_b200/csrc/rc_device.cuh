@@ -50,8 +50,9 @@ struct DLevel {
     int im, jm, km, maxs;
     int rx, ry, rz;           // ratio to the next (coarser) level
     unsigned mrx, mry, mrz;   // floor(2^32 / r) + 1 (0 for r = 1): (n + r - 1) / r as a multiply-high
-    const R *xu, *yu, *zu;    // faces
-    const uint16_t *P;        // table coordinate of every cell, i fastest (see cell_index)
+    const R *xu, *yu, *zu;    // faces (views into DSolve::faces)
+    const uint16_t *P;        // table coordinate of every cell, i fastest (see cell_index);
+                              // a view into DSolve::Pall
     const uint16_t *Pw[6];    // wall emission temperature coordinates (or null)
 };
 
@@ -78,6 +79,12 @@ struct DScalars {
 
 template <typename R>
 struct DSolve {
+    // what a step reads of its level, two 16-byte loads:
+    // lva = offsets of xu, yu, zu in faces and of the coordinates in Pall;
+    // lvb = (im, jm, km, maxs)
+    int4 lva[RC_MAX_LEVELS], lvb[RC_MAX_LEVELS];
+    const R *faces;           // every level's xu | yu | zu, one after the other
+    const uint16_t *Pall;     // every level's table coordinates, one after the other
     DLevel<R> lev[RC_MAX_LEVELS];
     int nlev;
     int imax, jmax, kmax, kloc, kfirst;
@@ -443,11 +450,14 @@ __device__ __forceinline__ void hit_wall(Ray<R> &r, const DSolve<R> &S, const DL
 // One ray-cell crossing (one iteration of the while loop of march_ray,
 // :252-656).
 template <typename R>
-__device__ __forceinline__ void march_step(Ray<R> &r, const DSolve<R> &S, const DLevel<R> &L) {
-    const R fxu = L.xu[r.ic - r.fx];
-    const R fyu = L.yu[r.jc - r.fy];
-    const R fzu = L.zu[r.kc - r.fz];
-    const int q = __ldg(&L.P[cell_index(r.ic, r.jc, r.kc, L.im, L.jm)]);
+__device__ __forceinline__ void march_step(Ray<R> &r, const DSolve<R> &S) {
+    // S lives in global memory (read-only during every kernel that steps)
+    const int4 A = __ldg(&S.lva[r.lev]);
+    const int4 B = __ldg(&S.lvb[r.lev]);
+    const R fxu = __ldg(S.faces + (A.x + r.ic - r.fx));
+    const R fyu = __ldg(S.faces + (A.y + r.jc - r.fy));
+    const R fzu = __ldg(S.faces + (A.z + r.kc - r.fz));
+    const int q = __ldg(S.Pall + (A.w + cell_index(r.ic, r.jc, r.kc, B.x, B.y)));
     const KIRow<R> row = load_row(r.kicol + (q >> 8));
     const R dsx = (fxu - r.xp) * r.isx;
     const R dsy = (fyu - r.yp) * r.isy;
@@ -485,7 +495,7 @@ __device__ __forceinline__ void march_step(Ray<R> &r, const DSolve<R> &S, const 
     r.jc += ax1 ? dlt : 0;
     r.kc += (axis == 2) ? dlt : 0;
     const int nidx = ax0 ? r.ic : (ax1 ? r.jc : r.kc);
-    const int lim = (ax0 ? L.im : (ax1 ? L.jm : L.km)) + 1;
+    const int lim = (ax0 ? B.x : (ax1 ? B.y : B.z)) + 1;
     if (nidx == 0 || nidx == lim) {
         const int w = 2 * axis + (nidx != 0);
         if (S.wtype[w] == 1) {
@@ -504,7 +514,7 @@ __device__ __forceinline__ void march_step(Ray<R> &r, const DSolve<R> &S, const 
                 r.zp = hi ? (R)0 : S.Lz;
             }
         } else {
-            hit_wall(r, S, L, w);
+            hit_wall(r, S, S.lev[r.lev], w);
         }
     }
     r.counter += 1;
@@ -523,7 +533,7 @@ __device__ __forceinline__ int coarse_index(int n, int r, unsigned m) {
 // last level spent).
 template <typename R>
 __device__ __forceinline__ bool level_advance(Ray<R> &r, const DSolve<R> &S) {
-    while (r.counter >= S.lev[r.lev].maxs) {
+    while (r.counter >= __ldg(&S.lvb[r.lev]).w) {
         if (r.lev >= S.nlev - 1) return false;
         const DLevel<R> &L = S.lev[r.lev];
         r.ic = coarse_index(r.ic, L.rx, L.mrx);

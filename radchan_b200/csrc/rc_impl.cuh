@@ -152,7 +152,8 @@ namespace rc_detail {
 
 template <typename R>
 struct Slot : SlotCommon {
-    std::vector<uint16_t *> d_levT;
+    uint16_t *d_levAll = nullptr;      // every level's table coordinates (one allocation)
+    std::vector<uint16_t *> d_levT;    // per-level views into d_levAll
     uint16_t *d_lw[RC_MAX_LEVELS][6] = {};
     uint16_t *d_Tw0[2] = {nullptr, nullptr};
     KIRow<R> *d_ki_grey = nullptr;
@@ -166,7 +167,9 @@ struct Slot : SlotCommon {
 template <typename R>
 struct Impl : ImplBase {
     rc_ctx *c = nullptr;
-    std::vector<R *> d_xu, d_yu, d_zu;
+    R *d_faces = nullptr;              // every level's xu | yu | zu (one allocation)
+    std::vector<R *> d_xu, d_yu, d_zu; // per-level views into d_faces
+    std::vector<int> face_off, lev_off;  // per-level offsets in d_faces / Slot::d_levAll
     R *d_xc = nullptr, *d_yc = nullptr, *d_zc = nullptr;
     R *d_kt = nullptr, *d_Ibt = nullptr, *d_probg = nullptr, *d_prob = nullptr, *d_probq = nullptr;
     R *d_Ibw = nullptr, *d_Tnb = nullptr, *d_kP = nullptr, *d_wvl = nullptr, *d_wvr = nullptr, *d_wvc = nullptr;
@@ -228,7 +231,8 @@ struct Impl : ImplBase {
             dfree(s.d_counter);
             dfree(s.d_out);
             hfree(s.h_out);
-            for (auto &p : s.d_levT) dfree(p);
+            dfree(s.d_levAll);
+            s.d_levT.clear();
             for (int l = 0; l < RC_MAX_LEVELS; ++l)
                 for (int w = 0; w < 6; ++w) dfree(s.d_lw[l][w]);
             dfree(s.d_Tw0[0]);
@@ -251,9 +255,7 @@ struct Impl : ImplBase {
             if (s.st) cudaStreamDestroy(s.st);
         }
         slots.clear();
-        for (auto &p : d_xu) dfree(p);
-        for (auto &p : d_yu) dfree(p);
-        for (auto &p : d_zu) dfree(p);
+        dfree(d_faces);
         d_xu.clear();
         d_yu.clear();
         d_zu.clear();
@@ -278,12 +280,28 @@ struct Impl : ImplBase {
         d_xu.assign(nl, nullptr);
         d_yu.assign(nl, nullptr);
         d_zu.assign(nl, nullptr);
-        for (int l = 0; l < nl; ++l) {
-            const GridLevel &g = c->grid[l];
-            int rc = upload(d_xu[l], g.xu, err_);
-            if (!rc) rc = upload(d_yu[l], g.yu, err_);
-            if (!rc) rc = upload(d_zu[l], g.zu, err_);
+        face_off.assign(nl, 0);
+        lev_off.assign(nl, 0);
+        {
+            std::vector<float> faces;
+            long long po = 0;
+            for (int l = 0; l < nl; ++l) {
+                const GridLevel &g = c->grid[l];
+                face_off[l] = (int)faces.size();
+                faces.insert(faces.end(), g.xu.begin(), g.xu.end());
+                faces.insert(faces.end(), g.yu.begin(), g.yu.end());
+                faces.insert(faces.end(), g.zu.begin(), g.zu.end());
+                lev_off[l] = (int)po;
+                po += (long long)p.maxi[l] * p.maxj[l] * p.maxk[l];
+                if (po > 0x7fffffffLL) return set_err(err_, RC_E_INVALID, "grid too large for 32-bit level offsets");
+            }
+            int rc = upload(d_faces, faces, err_);
             if (rc) return rc;
+            for (int l = 0; l < nl; ++l) {
+                d_xu[l] = d_faces + face_off[l];
+                d_yu[l] = d_xu[l] + (p.maxi[l] + 1);
+                d_zu[l] = d_yu[l] + (p.maxj[l] + 1);
+            }
         }
         int rc = upload(d_xc, c->grid[0].x, err_);
         if (!rc) rc = upload(d_yc, c->grid[0].y, err_);
@@ -328,6 +346,13 @@ struct Impl : ImplBase {
             RC_CK(cudaHostAlloc((void **)&s.h_desc, sizeof(DSolve<R>), cudaHostAllocDefault));
             // multigrid pyramid and wall emission arrays
             s.d_levT.assign(nl, nullptr);
+            {
+                long long tot = 0;
+                for (int l = 0; l < nl; ++l) tot += (long long)p.maxi[l] * p.maxj[l] * p.maxk[l];
+                RC_CK(cudaMalloc((void **)&s.d_levAll, tot * sizeof(uint16_t)));
+                RC_CK(cudaMemset(s.d_levAll, 0, tot * sizeof(uint16_t)));
+                for (int l = 0; l < nl; ++l) s.d_levT[l] = s.d_levAll + lev_off[l];
+            }
             LevelJobs &J = s.jobs;
             memset(&J, 0, sizeof(J));
             auto add_job = [&](void *dst, int type, int l, int face, long long n) {
@@ -347,8 +372,6 @@ struct Impl : ImplBase {
             };
             for (int l = 0; l < nl; ++l) {
                 const long long n = (long long)p.maxi[l] * p.maxj[l] * p.maxk[l];
-                RC_CK(cudaMalloc((void **)&s.d_levT[l], n * sizeof(uint16_t)));
-                RC_CK(cudaMemset(s.d_levT[l], 0, n * sizeof(uint16_t)));
                 add_job(s.d_levT[l], 0, l, 0, n);
                 for (int w = 0; w < 6; ++w) {
                     const int t = c->wt[w];
@@ -556,6 +579,8 @@ struct Impl : ImplBase {
             L.yu = d_yu[l];
             L.zu = d_zu[l];
             L.P = s.d_levT[l];
+            d.lva[l] = make_int4(face_off[l], face_off[l] + L.im + 1, face_off[l] + L.im + 1 + L.jm + 1, lev_off[l]);
+            d.lvb[l] = make_int4(L.im, L.jm, L.km, L.maxs);
             for (int w = 0; w < 6; ++w) L.Pw[w] = s.d_lw[l][w];
         }
         d.imax = p.imax;
@@ -582,6 +607,8 @@ struct Impl : ImplBase {
         d.Lz = (R)p.Lz;
         d.toll = (R)p.toll;
         d.tollS = (R)p.tollS;
+        d.faces = d_faces;
+        d.Pall = s.d_levAll;
         d.xc = d_xc;
         d.yc = d_yc;
         d.zc = d_zc;

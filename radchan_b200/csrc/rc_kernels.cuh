@@ -303,13 +303,9 @@ __global__ void k_trace(const DSolve<R> *Sp, int n, const rc_bundle_id *ids, rc_
                         int *cells) {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= n) return;
-    DSolve<R> S = *Sp;
-    const DScalars *sc = S.sc;
-    S.Pm = sc->Pm;
-    S.Ibmax_f = (R)sc->Ibmax_f;
-    S.Ibmax_w0 = (R)sc->Ibmax_w[0];
-    S.Ibmax_w1 = (R)sc->Ibmax_w[1];
-    S.row = sc->row;
+    // the descriptor of a finished solve, its run-time fields patched by
+    // k_patch_desc before the march
+    const DSolve<R> &S = *Sp;
     const rc_bundle_id id = ids[t];
     rc_trace_rec rec;
     rec.nb = rec.g = -1;
@@ -338,7 +334,7 @@ __global__ void k_trace(const DSolve<R> *Sp, int n, const rc_bundle_id *ids, rc_
                 c[2] = r.jc;
                 c[3] = r.kc;
             }
-            march_step(r, S, S.lev[r.lev]);
+            march_step(r, S);
             ns++;
             active = r.tra > r.tol;
             if (active) active = level_advance(r, S);

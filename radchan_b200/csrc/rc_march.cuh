@@ -255,7 +255,7 @@ __global__ void __launch_bounds__(256, MINB) k_march(MarchArgs a) {
             for (;;) {
                 bool fin = false;
                 if (active) {
-                    march_step(r, S, S.lev[r.lev]);
+                    march_step(r, S);
                     nsteps++;
                     bool done = !(r.tra > r.tol);
                     if (!done) done = !level_advance(r, S);
