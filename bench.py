@@ -2,8 +2,9 @@
 
 Default workload: narrow-band correlated-k 64^3 channel (100 bands x 8 g,
 64 temperatures, 3 multigrid levels 64/32/16 with maxs 5/5/1e5,
-photmax 256, nVar 4, band-sorted order, adiabatic west wall with wall-flux
-kernel), seeded synthetic field and tables.  One step = one full solve.
+photmax 256, nVar 4, srt 1 in the parameter set, adiabatic west wall with
+wall-flux kernel), seeded synthetic field and tables.  One step = one full
+solve.
 
   value  photon bundles/s with the field already in HBM (device time of the
          solve: copy-in, set-up, march, tally), max over ranks, summed over
@@ -48,8 +49,9 @@ BUNDLE_METRIC = "bundles/s & solves/s at 1% MC std, batched/served vs plain; ser
 
 # DRAM bytes (read + write) of one k_march launch, from the ncu capture
 # summarised in profiles/k_march_nb64_photmax64_full.txt
-# (dram__bytes_read.sum + dram__bytes_write.sum).  The march's working set (temperature pyramid and
-# tables, ~1.5 MB) is L2-resident, so the traffic does not grow with photmax.
+# (dram__bytes_read.sum + dram__bytes_write.sum).  The march's working set
+# (temperature pyramid and tables, ~1.5 MB) is L2-resident, so the traffic
+# does not grow with photmax.
 K_MARCH_TRAFFIC = {"nb64": 990208 + 17664}
 
 
