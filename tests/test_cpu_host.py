@@ -74,6 +74,34 @@ def test_synthetic_tables_are_consistent():
     assert np.all(t["kP"] > 0)
 
 
+def _i_black(T, nu):
+    """Spectral blackbody intensity, nu in cm^-1 (nbcorrk/ckdist_hitran_part.cpp:229-233)."""
+    c1, c2 = 3.741771790075259e-16, 0.014387741858429
+    return c1 * (nu * 100.0) ** 3 / (np.pi * np.expm1(c2 * nu * 100.0 / T))
+
+
+@pytest.mark.parametrize("nB,nQ,nT", [(50, 8, 32), (7, 4, 3), (1, 1, 2)])
+def test_synthetic_tables_follow_reference_cdf_law(nB, nQ, nT):
+    """The band and g cumulative probabilities and the Planck-mean
+    coefficient restated from nbcorrk/calc_prob.cpp:54-116 on the table's own
+    k, weights and band edges: band CDF ~ sum_g w_g k_bg I_b(T, nu_b) dnu_b,
+    g CDF within a band ~ w_g k_bg, kP = pi sum k I_b dnu / (sigma T^4)."""
+    t = W.tables_nb(nB=nB, nQ=nQ, nT=nT).arrays()
+    kq = t["kq"].astype(np.float64).reshape(nB, nT, nQ)
+    wq = t["wq"].astype(np.float64)
+    nu = t["wvc"].astype(np.float64)
+    dnu = (t["wvr"].astype(np.float64) - t["wvl"].astype(np.float64)) * 100.0
+    sigma = 5.670373e-08
+    for i, T in enumerate(t["Tnb"].astype(np.float64)):
+        k = kq[:, i, :]                                           # [nB, nQ]
+        pb = (k * wq).sum(axis=1) * _i_black(T, nu) * dnu         # calc_prob.cpp:73-76
+        np.testing.assert_allclose(t["prob"][i], np.cumsum(pb) / pb.sum(), rtol=2e-5, atol=1e-9)
+        cg = np.cumsum(k * wq, axis=1)                            # calc_prob.cpp:97-116
+        np.testing.assert_allclose(t["probg"][i], cg / cg[:, -1:], rtol=2e-6, atol=1e-9)
+        kP = np.pi * pb.sum() / (sigma * T ** 4)                  # calc_prob.cpp:54-56
+        np.testing.assert_allclose(t["kP"][i], kP, rtol=2e-5)
+
+
 def test_reference_table_files_round_trip(tmp_path):
     ts = W.tables_nb(nB=12, nQ=8, nT=16)
     ts.write_dir(tmp_path)
