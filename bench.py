@@ -21,7 +21,10 @@ Legs on one GPU (skipped with --no-legs):
          narrow-band 20-100 bands, photmax 32/128/512): plain one solve per
          launch vs one persistent launch from a CUDA graph vs the
          continuous-batching server, solves/s by wall clock;
-  batched_small  the same with edges 16..32 and photmax 32/128.
+  batched_small  the same with edges 16..32 and photmax 32/128;
+  dns_source  the DNS coupling kernel (Q, sigma -> Qnew, Varnew, Knew,
+         Gnew) on the 192x128x128 channel: device time per launch, HBM
+         roofline, host entry point time, CPU restatement time.
 
 --serve runs the open-loop serving benchmark instead (Poisson arrivals at
 --load x measured capacity, tolerance-driven photmax, p50/p99 latency);
@@ -246,6 +249,77 @@ def leg_at_tolerance(p, tabs, T, rel0, dev, flush, tol=0.01, steps=2):
     sec = sum(ms) / 1000.0
     return {"tolerance": tol, "photmax": q.photmax, "rel_std_maxq": rel, "ms_per_solve": 1000 * sec / steps,
             "solves_per_s": steps / sec, "bundles_per_s": bundles / sec, "steps": steps}
+
+
+def leg_dns_source(dev, flush, reps=20, cpu=True):
+    """The DNS coupling kernel (k_dns_source: GET_RESULTS + fix_rad +
+    fix_kappa + the Gnew loop of src/dns/channel.f:249-266) on the
+    192x128x128 channel (the largest grid of the workload family), full
+    j pencil: device time per launch on the launching stream with L2
+    flushed before each launch, HBM roofline at 48 algorithmic bytes per
+    output cell (float Q and sigma 8, double T1 8, four double outputs 32);
+    the host entry point (T1 in, four arrays out over PCIe) by wall clock;
+    the CPU restatement on the same arrays."""
+    import torch
+
+    from radchan_b200 import api
+    from radchan_b200 import workloads as W
+    p = W.config_precision(photmax=1, nVar=2)
+    tabs = W.tables_nb()
+    a = tabs.arrays()
+    Tin = 955.0
+    cpl = api.DnsCoupling(Tin=Tin, Height=0.5, underrelax=1.0, Tnb=a["Tnb"].astype(np.float64),
+                          kP=a["kP"].astype(np.float64) * 0.5)
+    T1 = W.channel_field(p).astype(np.float64) / Tin
+    T = api.field_from_dns(T1, Tin)
+    s = api.Solver(p, tabs, device=dev)
+    tshape, oshape = cpl.pencil_shapes(p)
+    cuda = torch.device("cuda:%d" % dev)
+    T1d = torch.from_numpy(np.ascontiguousarray(T1)).to(cuda)
+    outs = [torch.empty(oshape, dtype=torch.float64, device=cuda) for _ in range(4)]
+    cnt = torch.zeros(1, dtype=torch.int64, device=cuda)
+    stream = torch.cuda.current_stream(cuda)
+    t = s.solve_async(T)
+    s.wait_device(t)
+    ptrs = [o.data_ptr() for o in outs]
+    for _ in range(3):
+        s.dns_source_device(t, cpl, T1d.data_ptr(), *ptrs, cnt.data_ptr(), stream=stream.cuda_stream)
+    ms = []
+    for _ in range(reps):
+        flush.zero_()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        s.dns_source_device(t, cpl, T1d.data_ptr(), *ptrs, cnt.data_ptr(), stream=stream.cuda_stream)
+        e1.record(stream)
+        e1.synchronize()
+        ms.append(e0.elapsed_time(e1))
+    r = s.collect(t, want64=False)
+    n_out = int(np.prod(oshape))
+    sec = sum(ms) / 1000.0 / reps
+    peak, peak_kind = peaks()
+    achieved = 48.0 * n_out / sec / 1e9
+    # host entry point: pencil in, four arrays out, per call after the solve
+    host_ms = []
+    for _ in range(3):
+        t = s.solve_async(T)
+        s.wait_device(t)
+        t0 = time.perf_counter()
+        s.dns_source(t, cpl, T1)
+        host_ms.append(1000 * (time.perf_counter() - t0))
+    s.close()
+    out = {"kernel": "k_dns_source", "grid": [p.imax, p.jmax, p.kmax], "cells": n_out, "launches": reps,
+           "ms_per_launch": 1000 * sec,
+           "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                        "peak_source": peak_kind, "algorithmic_bytes_per_cell": 48},
+           "host_entry_ms": min(host_ms), "host_entry_bytes": int(T1.nbytes + 32 * n_out),
+           "l2": "flushed before each launch"}
+    if cpu:
+        from oracle import dns as OD
+        t0 = time.perf_counter()
+        OD.dns_source(r.Q, r.sigma, T1, Tin, cpl.Height, cpl.underrelax, cpl.stefan, cpl.Tnb, cpl.kP, 1, p.jmax)
+        out["cpu_baseline"] = {"ms": 1000 * (time.perf_counter() - t0), "cores": 1, "kind": "port",
+                               "sample": "the whole pencil, numpy restatement of fixvar.f/channel.f"}
+    return out
 
 
 def batch_setup(dev, n=64, edges=(16, 24, 32, 48, 64, 96), photmaxes=(32, 128, 512)):
@@ -552,6 +626,7 @@ def run_ours(args, ws, rank, local):
         # the same recipe restricted to small problems (edges 16-32, photmax
         # 32/128), where one solve does not fill the GPU
         line["batched_small"] = leg_batched(dev, edges=(16, 24, 32), photmaxes=(32, 128))
+        line["dns_source"] = leg_dns_source(dev, flush, cpu=not args.no_cpu_baseline)
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         cb = cpu_sample(p, tabs, T, seconds=args.ref_seconds)
         line["cpu_baseline"] = {"value": cb["bundles"] / cb["seconds"], "unit": "bundles/s",

@@ -302,6 +302,49 @@ int rc_server_quanta(rc_server *s, long long *quanta);
 int rc_server_set_policy(rc_server *s, int policy);
 int rc_server_destroy(rc_server *s);
 
+/* ---------------- DNS coupling ---------------- */
+
+/* What the channel DNS does with a finished solve before its energy
+ * equation uses it (src/dns/channel.f:249-266): GET_RESULTS, then fix_rad
+ * (fixvar.f:179-242: Q and sigma over stefan Tin^4, wall fluxes also over
+ * Height, the DNS rank's j pencil cut out), fix_kappa (fixvar.f:16-43:
+ * Planck-mean coefficient at T1 Tin by linear_int), then
+ * Qnew *= underrelax and Gnew = 4 T1^4 - Qnew / Knew. */
+#define RC_DNS_MAX_T 128
+typedef struct rc_dns_coupling {
+    double Tin;          /* temperature scale, K: T = T1 Tin (channel.f:111) */
+    double Height;       /* divides the wall fluxes (fixvar.f:223-224; channel.f:106) */
+    double underrelax;   /* multiplies Qnew before Gnew is formed (channel.f:263) */
+    double stefan;       /* Stefan-Boltzmann constant of the DNS (param.txt:41: 5.67e-08) */
+    int nTemp;           /* rows of Tnb and kP, 2..RC_DNS_MAX_T */
+    const double *Tnb;   /* [nTemp] table temperatures, K, ascending with a uniform step >= 1 K */
+    const double *kP;    /* [nTemp] Planck-mean coefficient already times Height (read_kP, fixvar.f:1-14) */
+    int jstart, jend;    /* 1-based global j range of the DNS pencil (xstart(2), xend(2)) */
+} rc_dns_coupling;
+/* Wait for a ticket and write the DNS source terms of the pencil
+ * j = jstart..jend (jn = jend - jstart + 1), k = 1..kloc of the solve:
+ *   Qnew   = Q / stefan / Tin^4 (walls i = 0, imax+1: then / Height), x underrelax
+ *   Varnew = sigma / stefan / Tin^4
+ *   Knew   = kP at T1 Tin, row t = int(T1 Tin - Tnb[0]) / int(Tnb[1] - Tnb[0])
+ *            (the truncating rule of linear_int, fixvar.f:35-43)
+ *   Gnew   = 4 T1^4 - Qnew / Knew   (T1^4 evaluated as (T1 T1)(T1 T1))
+ * with Q and sigma exactly the values rc_collect / get_results_ give.
+ * T1 is the DNS's nondimensional temperature pencil (0:imax+1, 0:jn+1,
+ * 0:kloc+1), i fastest; the four outputs are (0:imax+1, jn, kloc) doubles.
+ * Where the row falls outside 0..nTemp-2 (the reference reads past its table
+ * there) the end interval is extended and the cell is counted in
+ * *n_clamped (optional).  The ticket is consumed, as by rc_collect. */
+int rc_dns_source(rc_ctx *ctx, rc_ticket ticket, const rc_dns_coupling *cfg, const double *T1,
+                  double *Qnew, double *Varnew, double *Knew, double *Gnew, long long *n_clamped);
+/* The same on device arrays, enqueued on `stream` (a cudaStream_t; NULL:
+ * the solve's own stream) behind the solve; returns at once.  The ticket
+ * stays valid (collect or release it afterwards) and the next solve in its
+ * slot waits for this kernel.  n_clamped_dev (optional) is a device
+ * counter that the kernel adds to. */
+int rc_dns_source_device(rc_ctx *ctx, rc_ticket ticket, const rc_dns_coupling *cfg, const double *T1_dev,
+                         double *Qnew_dev, double *Varnew_dev, double *Knew_dev, double *Gnew_dev,
+                         unsigned long long *n_clamped_dev, void *stream);
+
 /* ---------------- reference-compatible entry points ---------------- */
 
 /* Configure the process-wide context used by mc_gpu_/get_results_.
@@ -317,6 +360,11 @@ int rc_legacy_release(void);
 void mc_gpu_(float *T, int *zstart, int *rank);
 /* mc_gpu_noint.cu:876 -- waits, then fills Q and sigma (Fortran layout). */
 void get_results_(float *Q, float *sigma, int *rank);
+/* channel.f:252-266 in one call: waits for the pending mc_gpu_ launch and
+ * writes the DNS source terms as rc_dns_source does (replaces GET_RESULTS,
+ * fix_rad, fix_kappa and the Gnew loop). */
+int rc_legacy_source(const rc_dns_coupling *cfg, const double *T1, double *Qnew, double *Varnew,
+                     double *Knew, double *Gnew, long long *n_clamped);
 
 #ifdef __cplusplus
 }

@@ -90,6 +90,15 @@ class RcResultInfo(C.Structure):
                 ("photmax", C.c_int), ("rel_std_maxq", C.c_float), ("status", C.c_int)]
 
 
+RC_DNS_MAX_T = 128
+
+
+class RcDnsCoupling(C.Structure):
+    _fields_ = [("Tin", C.c_double), ("Height", C.c_double), ("underrelax", C.c_double), ("stefan", C.c_double),
+                ("nTemp", C.c_int), ("Tnb", C.POINTER(C.c_double)), ("kP", C.POINTER(C.c_double)),
+                ("jstart", C.c_int), ("jend", C.c_int)]
+
+
 # (name, restype, argtypes) for every function declared in include/radchan.h
 _VP = C.c_void_p
 _I = C.c_int
@@ -133,6 +142,10 @@ _SIGS = [
     ("rc_server_set_quantum", _I, [_VP, C.c_longlong]),
     ("rc_server_quanta", _I, [_VP, C.POINTER(C.c_longlong)]),
     ("rc_server_set_policy", _I, [_VP, _I]),
+    ("rc_dns_source", _I, [_VP, C.c_int32, C.POINTER(RcDnsCoupling), _DP, _DP, _DP, _DP, _DP,
+                           C.POINTER(C.c_longlong)]),
+    ("rc_dns_source_device", _I, [_VP, C.c_int32, C.POINTER(RcDnsCoupling), _VP, _VP, _VP, _VP, _VP, _VP, _VP]),
+    ("rc_legacy_source", _I, [C.POINTER(RcDnsCoupling), _DP, _DP, _DP, _DP, _DP, C.POINTER(C.c_longlong)]),
     ("rc_legacy_configure", _I, [C.POINTER(RcParams), C.POINTER(RcTables)]),
     ("rc_legacy_release", _I, []),
     ("mc_gpu_", None, [_FP, C.POINTER(C.c_int), C.POINTER(C.c_int)]),

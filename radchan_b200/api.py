@@ -145,6 +145,61 @@ def result_shape(p):
 
 
 @dataclass
+class DnsCoupling:
+    """How the channel DNS turns a solve into its energy-equation source
+    (src/dns/channel.f:249-266, fixvar.f:16-43 and :179-242); see
+    rc_dns_coupling in radchan.h."""
+    Tin: float                 # temperature scale, K (T = T1 * Tin)
+    Height: float              # divides the wall fluxes
+    underrelax: float          # multiplies Qnew before Gnew is formed
+    Tnb: np.ndarray            # table temperatures, K, uniform step >= 1 K
+    kP: np.ndarray             # Planck-mean coefficient times Height
+    jstart: int = 1            # 1-based global j range of the DNS pencil
+    jend: int = -1             # -1: jmax
+    stefan: float = 5.67e-08   # the DNS's constant (src/dns/param.txt:41)
+
+    def struct(self, jmax):
+        self._Tnb = np.ascontiguousarray(self.Tnb, np.float64)
+        self._kP = np.ascontiguousarray(self.kP, np.float64)
+        dp = C.POINTER(C.c_double)
+        return L.RcDnsCoupling(self.Tin, self.Height, self.underrelax, self.stefan, len(self._Tnb),
+                               self._Tnb.ctypes.data_as(dp), self._kP.ctypes.data_as(dp), self.jstart,
+                               jmax if self.jend < 0 else self.jend)
+
+    def pencil_shapes(self, p):
+        """(T1 shape, output shape) of the pencil, numpy order (k, j, i)."""
+        kl = p.kmax // p.p_col
+        jn = (p.jmax if self.jend < 0 else self.jend) - self.jstart + 1
+        return (kl + 2, jn + 2, p.imax + 2), (kl, jn, p.imax + 2)
+
+
+def field_from_dns(T1, Tin):
+    """The solver's float field from the DNS's nondimensional double T1
+    (whole field with ghosts, numpy order (k, j, i)): real(T1*Tin, 4), the
+    conversion of bcastArr (src/dns/routine.f90:205-209).  bcastArr leaves
+    the j and k ghost planes of its output untouched; here they come from
+    T1's own halo."""
+    return (np.asarray(T1, np.float64) * Tin).astype(np.float32)
+
+
+def read_planck_mean(path, n, height):
+    """read_kP (src/dns/fixvar.f:1-14): Tnb and kP * height from the first n
+    rows of planck-mean.txt ("T kP kR kM" per row)."""
+    rows = []
+    with open(path) as f:
+        for line in f:
+            v = line.split()
+            if len(v) >= 2:
+                rows.append((float(v[0]), float(v[1])))
+            if len(rows) == n:
+                break
+    if len(rows) < n:
+        raise L.RadChanError(-4, "%s has fewer than %d rows" % (path, n))
+    a = np.array(rows, np.float64)
+    return a[:, 0].copy(), a[:, 1] * height
+
+
+@dataclass
 class Result:
     Q: np.ndarray          # Fortran-layout float result (kloc+2, jmax+2, imax+2)
     sigma: np.ndarray
@@ -220,6 +275,31 @@ class Solver:
 
     def solve(self, T, zstart=1, want64=True) -> Result:
         return self.collect(self.solve_async(T, zstart), want64)
+
+    def dns_source(self, ticket: int, cpl: DnsCoupling, T1: np.ndarray):
+        """Wait for a ticket and return the DNS source terms of the pencil
+        (rc_dns_source): dict of Qnew, Varnew, Knew, Gnew as (kloc, jn,
+        imax+2) float64 arrays and n_clamped.  The ticket is consumed."""
+        s = cpl.struct(self.p.jmax)
+        tshape, oshape = cpl.pencil_shapes(self.p)
+        T1 = np.ascontiguousarray(T1, np.float64)
+        assert T1.shape == tshape, (T1.shape, tshape)
+        out = {k: np.empty(oshape, np.float64) for k in ("Qnew", "Varnew", "Knew", "Gnew")}
+        n = C.c_longlong()
+        dp = lambda a: a.ctypes.data_as(C.POINTER(C.c_double))
+        L.check(L.lib().rc_dns_source(self.ctx, ticket, C.byref(s), dp(T1), dp(out["Qnew"]), dp(out["Varnew"]),
+                                      dp(out["Knew"]), dp(out["Gnew"]), C.byref(n)), self.ctx)
+        out["n_clamped"] = n.value
+        return out
+
+    def dns_source_device(self, ticket: int, cpl: DnsCoupling, T1_dev: int, Qnew_dev: int, Varnew_dev: int,
+                          Knew_dev: int, Gnew_dev: int, n_clamped_dev: int = 0, stream: int = 0):
+        """rc_dns_source_device: the same on device pointers, enqueued on
+        `stream` (0: the solve's stream); returns at once, the ticket stays."""
+        s = cpl.struct(self.p.jmax)
+        v = lambda x: C.c_void_p(x) if x else None
+        L.check(L.lib().rc_dns_source_device(self.ctx, ticket, C.byref(s), v(T1_dev), v(Qnew_dev), v(Varnew_dev),
+                                             v(Knew_dev), v(Gnew_dev), v(n_clamped_dev), v(stream)), self.ctx)
 
     def trace(self, ticket, ids, max_cells=0):
         n = len(ids)

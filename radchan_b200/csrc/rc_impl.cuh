@@ -112,6 +112,7 @@ struct ImplBase {
 struct SlotCommon {
     cudaStream_t st = nullptr;
     cudaEvent_t e0 = nullptr, e1 = nullptr, e_march0 = nullptr, e_march1 = nullptr;
+    cudaEvent_t e_dns = nullptr;  // end of a DNS-source kernel on another stream
     float *d_T = nullptr, *h_T = nullptr;
     DScalars *d_sc = nullptr, *h_sc = nullptr;
     double *d_partial = nullptr;
@@ -143,6 +144,10 @@ struct rc_ctx {
     int rpt = 8, block = 256, sort = 0, minb = 3;
     int num_sms = 148;
     bool has_tables = false;
+    // DNS-coupling scratch (rc_dns_source): T1 pencil + four outputs, and a counter
+    double *d_dns = nullptr;
+    size_t dns_cap = 0;
+    unsigned long long *d_dns_n = nullptr;
     // precision-specific state
     void *impl = nullptr;  // Impl<float> or Impl<double>
     int dbl = 0;
@@ -252,6 +257,7 @@ struct Impl : ImplBase {
             if (s.e1) cudaEventDestroy(s.e1);
             if (s.e_march0) cudaEventDestroy(s.e_march0);
             if (s.e_march1) cudaEventDestroy(s.e_march1);
+            if (s.e_dns) cudaEventDestroy(s.e_dns);
             if (s.st) cudaStreamDestroy(s.st);
         }
         slots.clear();

@@ -4,7 +4,10 @@
 //   mc_gpu_      (src/montecarlo/mc_gpu_noint.cu:660): copy T, launch, return
 //                without waiting;
 //   get_results_ (src/montecarlo/mc_gpu_noint.cu:876): wait, fill Q and the
-//                Monte Carlo standard deviation in the Fortran layout.
+//                Monte Carlo standard deviation in the Fortran layout;
+//   rc_legacy_source (src/dns/channel.f:252-266): wait, and write the DNS's
+//                Qnew, Varnew, Knew, Gnew (GET_RESULTS + fix_rad +
+//                fix_kappa + the Gnew loop, rc_dns.cu).
 //
 // The reference configures the solver at compile time and re-reads its
 // tables on every call; here the first mc_gpu_ configures the context from
@@ -124,6 +127,19 @@ void get_results_(float *Q, float *sigma, int *rank) {
     int rc = rc_collect(g_ctx, g_ticket, Q, sigma, nullptr, nullptr, nullptr, nullptr);
     g_have_ticket = 0;
     if (rc) report("get_results_");
+}
+
+int rc_legacy_source(const rc_dns_coupling *cfg, const double *T1, double *Qnew, double *Varnew, double *Knew,
+                     double *Gnew, long long *n_clamped) {
+    std::lock_guard<std::mutex> lk(g_mu);
+    if (!g_ctx || !g_have_ticket) {
+        fprintf(stderr, "radchan: rc_legacy_source called without a pending mc_gpu_ launch\n");
+        return RC_E_STATE;
+    }
+    int rc = rc_dns_source(g_ctx, g_ticket, cfg, T1, Qnew, Varnew, Knew, Gnew, n_clamped);
+    g_have_ticket = 0;
+    if (rc) report("rc_legacy_source");
+    return rc;
 }
 
 }  // extern "C"

@@ -228,6 +228,8 @@ int rc_destroy(rc_ctx *c) {
         if (c->dbl) delete static_cast<Impl<double> *>(c->impl);
         else delete static_cast<Impl<float> *>(c->impl);
     }
+    if (c->d_dns) cudaFree(c->d_dns);
+    if (c->d_dns_n) cudaFree(c->d_dns_n);
     delete c;
     return RC_OK;
 }
