@@ -54,10 +54,19 @@ module radchan_mod
     type(c_ptr) :: Tnb, kP, wvl, wvr, wvc, kavg, kq, prob, probg, wq
   end type rc_tables
 
+  ! mirror of struct rc_dns_coupling: what the DNS does with a finished
+  ! solve (channel.f:249-266, fixvar.f:16-43 and :179-242)
+  type, bind(C), public :: rc_dns_coupling
+    real(c_double) :: Tin, Height, underrelax, stefan
+    integer(c_int) :: nTemp
+    type(c_ptr) :: Tnb, kP        ! c_loc of real(8) arrays(nTemp); kP already times Height
+    integer(c_int) :: jstart, jend
+  end type rc_dns_coupling
+
   public :: mc_gpu, get_results
   public :: rc_params_from_headers, rc_create, rc_set_tables, rc_tables_read_dir, rc_tables_view
   public :: rc_tables_free, rc_solve_async, rc_collect, rc_destroy, rc_last_error
-  public :: rc_legacy_configure, c_string
+  public :: rc_legacy_configure, rc_dns_source, rc_legacy_source, c_string
 
   interface
     ! the reference's entry points (mc_gpu_noint.cu:660, :876)
@@ -145,6 +154,30 @@ module radchan_mod
       type(rc_params), intent(in) :: p
       type(c_ptr), value :: tables
     end function rc_legacy_configure
+
+    ! GET_RESULTS + fix_rad + fix_kappa + the Gnew loop for a ticket:
+    ! T1(0:i1, 0:jn+1, 0:kloc+1) real(8) nondimensional; Qnew, Varnew, Knew,
+    ! Gnew(0:i1, jn, kloc) real(8); n_clamped: c_loc of an integer(8) or c_null_ptr
+    integer(c_int) function rc_dns_source(ctx, ticket, cfg, T1, Qnew, Varnew, Knew, Gnew, n_clamped) &
+        bind(C, name="rc_dns_source")
+      import :: c_double, c_int, c_int32_t, c_ptr, rc_dns_coupling
+      type(c_ptr), value :: ctx
+      integer(c_int32_t), value :: ticket
+      type(rc_dns_coupling), intent(in) :: cfg
+      real(c_double), intent(in) :: T1(*)
+      real(c_double), intent(inout) :: Qnew(*), Varnew(*), Knew(*), Gnew(*)
+      type(c_ptr), value :: n_clamped
+    end function rc_dns_source
+
+    ! the same for the pending mc_gpu launch (replaces channel.f:252-266)
+    integer(c_int) function rc_legacy_source(cfg, T1, Qnew, Varnew, Knew, Gnew, n_clamped) &
+        bind(C, name="rc_legacy_source")
+      import :: c_double, c_int, c_ptr, rc_dns_coupling
+      type(rc_dns_coupling), intent(in) :: cfg
+      real(c_double), intent(in) :: T1(*)
+      real(c_double), intent(inout) :: Qnew(*), Varnew(*), Knew(*), Gnew(*)
+      type(c_ptr), value :: n_clamped
+    end function rc_legacy_source
   end interface
 
 contains

@@ -81,7 +81,11 @@ def test_rows_outside_the_table_are_extended_and_counted():
     p, tabs, cpl, T1 = _problem()
     T = api.field_from_dns(T1, TIN)
     T1p = _pencil(T1, cpl, p).copy()
-    T1p[3, 4, 5] = 250.0 / TIN      # below Tnb[0] - 1 K
+    Tnb0, step = cpl.Tnb[0], cpl.Tnb[1] - cpl.Tnb[0]
+    # int(x0 - Tnb[0]) / int(step) truncates toward zero: up to one step
+    # below Tnb[0] still maps to row 0, two steps below does not
+    T1p[2, 4, 5] = (Tnb0 - 0.9 * step) / TIN
+    T1p[3, 4, 5] = (Tnb0 - 2.0 * step) / TIN
     T1p[4, 6, 7] = 2500.0 / TIN     # above the last row
     s = api.Solver(p, tabs)
     r = s.solve(T)
