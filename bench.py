@@ -278,21 +278,26 @@ def leg_dns_source(dev, flush, reps=20, cpu=True):
     T1d = torch.from_numpy(np.ascontiguousarray(T1)).to(cuda)
     outs = [torch.empty(oshape, dtype=torch.float64, device=cuda) for _ in range(4)]
     cnt = torch.zeros(1, dtype=torch.int64, device=cuda)
-    stream = torch.cuda.current_stream(cuda)
+    # a stream of its own: handle 0 (torch's legacy default stream) would
+    # select the solve's stream in rc_dns_source_device
+    stream = torch.cuda.Stream(device=cuda)
+    torch.cuda.synchronize(cuda)
     t = s.solve_async(T)
     s.wait_device(t)
     ptrs = [o.data_ptr() for o in outs]
-    for _ in range(3):
-        s.dns_source_device(t, cpl, T1d.data_ptr(), *ptrs, cnt.data_ptr(), stream=stream.cuda_stream)
-    ms = []
-    for _ in range(reps):
-        flush.zero_()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        s.dns_source_device(t, cpl, T1d.data_ptr(), *ptrs, cnt.data_ptr(), stream=stream.cuda_stream)
-        e1.record(stream)
-        e1.synchronize()
-        ms.append(e0.elapsed_time(e1))
+    with torch.cuda.stream(stream):
+        for _ in range(3):
+            s.dns_source_device(t, cpl, T1d.data_ptr(), *ptrs, cnt.data_ptr(), stream=stream.cuda_stream)
+        ms = []
+        for _ in range(reps):
+            flush.zero_()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            s.dns_source_device(t, cpl, T1d.data_ptr(), *ptrs, cnt.data_ptr(), stream=stream.cuda_stream)
+            e1.record(stream)
+            e1.synchronize()
+            ms.append(e0.elapsed_time(e1))
+    torch.cuda.synchronize(cuda)
     r = s.collect(t, want64=False)
     n_out = int(np.prod(oshape))
     sec = sum(ms) / 1000.0 / reps

@@ -337,7 +337,8 @@ typedef struct rc_dns_coupling {
 int rc_dns_source(rc_ctx *ctx, rc_ticket ticket, const rc_dns_coupling *cfg, const double *T1,
                   double *Qnew, double *Varnew, double *Knew, double *Gnew, long long *n_clamped);
 /* The same on device arrays, enqueued on `stream` (a cudaStream_t; NULL:
- * the solve's own stream) behind the solve; returns at once.  The ticket
+ * the solve's own stream -- the legacy default stream cannot be named)
+ * behind the solve; returns at once.  The ticket
  * stays valid (collect or release it afterwards) and the next solve in its
  * slot waits for this kernel.  n_clamped_dev (optional) is a device
  * counter that the kernel adds to. */

@@ -60,9 +60,12 @@ def test_device_and_host_entry_points_equal_oracle(jstart, jend, adiabe):
     T1d = torch.from_numpy(T1p).to(dev)
     outs = [torch.full(oshape, np.nan, dtype=torch.float64, device=dev) for _ in range(4)]
     cnt = torch.zeros(1, dtype=torch.int64, device=dev)
-    s.dns_source_device(t, cpl, T1d.data_ptr(), *[o.data_ptr() for o in outs], cnt.data_ptr(),
-                        stream=torch.cuda.current_stream().cuda_stream)
+    # a stream of the caller's: the kernel waits for the solve on it
+    side = torch.cuda.Stream(device=dev)
     torch.cuda.synchronize()
+    s.dns_source_device(t, cpl, T1d.data_ptr(), *[o.data_ptr() for o in outs], cnt.data_ptr(),
+                        stream=side.cuda_stream)
+    side.synchronize()
     r = s.collect(t)
     want = _oracle(r, T1p, cpl, p)
     got = dict(zip(("Qnew", "Varnew", "Knew", "Gnew"), (o.cpu().numpy() for o in outs)))
