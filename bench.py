@@ -662,6 +662,8 @@ def main():
                     help="skip the 1%%-tolerance and batched-mix legs (profiling runs)")
     ap.add_argument("--serve", action="store_true", help="open-loop serving run instead of the solve benchmark")
     ap.add_argument("--precision", action="store_true", help="FP32 march vs FP64 build study instead")
+    ap.add_argument("--dns-leg", dest="dns_leg", action="store_true",
+                    help="only the DNS coupling leg (profiling runs)")
     ap.add_argument("--serve-requests", dest="serve_requests", type=int, default=200)
     ap.add_argument("--serve-inflight", dest="serve_inflight", type=int, default=32)
     ap.add_argument("--policy", default="srpt", choices=["srpt", "fair"])
@@ -672,6 +674,13 @@ def main():
         run_serve(args, rank, local)
     elif args.precision:
         run_precision(args, rank, local)
+    elif args.dns_leg:
+        import torch
+        torch.cuda.set_device(local)
+        flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda:%d" % local)
+        leg = leg_dns_source(local, flush, reps=args.steps, cpu=not args.no_cpu_baseline)
+        if rank == 0:
+            print(json.dumps(leg), flush=True)
     elif args.impl == "reference":
         run_reference(args, ws, rank)
     else:
