@@ -34,13 +34,14 @@ struct DnsArgs {
     double stefan, Tin, Tin4, Height, underrelax;
     int imax, jmax, kloc, jstart, jn, west, east;
     int nT, dT;
+    unsigned long long Mnx, Mjn, MdT;  // fdiv multipliers of imax+2, jn, dT
     double Tnb[RC_DNS_MAX_T], kP[RC_DNS_MAX_T], slope[RC_DNS_MAX_T];
 };
 
-// One block iteration per (j, k) row of the pencil, threads along i: the
-// row's index arithmetic is done once, in 32 bits, and every load and store
-// of a warp is contiguous.
-__global__ void __launch_bounds__(128) k_dns_source(const __grid_constant__ DnsArgs a) {
+// One thread per output cell (grid-stride), i fastest, so every load and
+// store of a warp is contiguous; (i, j, k) and linear_int's row come from
+// exact multiply-high divisions (fdiv) instead of integer division.
+__global__ void __launch_bounds__(256) k_dns_source(const __grid_constant__ DnsArgs a) {
     __shared__ double sT[RC_DNS_MAX_T], sK[RC_DNS_MAX_T], sS[RC_DNS_MAX_T];
     for (int t = threadIdx.x; t < a.nT; t += blockDim.x) {
         sT[t] = a.Tnb[t];
@@ -49,55 +50,57 @@ __global__ void __launch_bounds__(128) k_dns_source(const __grid_constant__ DnsA
     }
     __syncthreads();
     const int nx = a.imax + 2;
-    const int nrows = a.jn * a.kloc;
+    const unsigned long long n = (unsigned long long)nx * a.jn * a.kloc;
     unsigned int clamped = 0;
-    for (int r = blockIdx.x; r < nrows; r += gridDim.x) {
-        const int jl = r % a.jn + 1;      // 1..jn, local to the pencil
-        const int kl = r / a.jn + 1;      // 1..kloc
-        const int jg = a.jstart + jl - 1;  // 1..jmax, the solve's j
-        const long long orow = (long long)r * nx;
-        const double *t1row = a.T1 + (long long)nx * (jl + (long long)(a.jn + 2) * kl);
+    for (unsigned long long c = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; c < n;
+         c += (unsigned long long)gridDim.x * blockDim.x) {
+        const unsigned long long r = fdiv(c, a.Mnx);  // (j, k) row
+        const int i = (int)(c - r * nx);
+        const unsigned long long k0 = fdiv(r, a.Mjn);
+        const int jl = (int)(r - k0 * a.jn) + 1;  // 1..jn, local to the pencil
+        const int kl = (int)k0 + 1;               // 1..kloc
+        const int jg = a.jstart + jl - 1;         // 1..jmax, the solve's j
         const long long wcell = (long long)(kl - 1) * a.jmax + (jg - 1);
-        const float *qrow = a.Qc + wcell * a.imax;  // fluid cell i at qrow[i - 1]
-        const float *srow = a.Sc + wcell * a.imax;
-        for (int i = threadIdx.x; i < nx; i += blockDim.x) {
-            const long long c = orow + i;
-            const bool wall = (i == 0) || (i == nx - 1);
-            float q = 0.f, s = 0.f;
-            if (wall) {
-                // get_results_ writes 0 on a wall whose flux is not computed
-                if (i == 0 ? a.west : a.east) {
-                    const long long w = (i == 0 ? 0LL : (long long)a.jmax * a.kloc) + wcell;
-                    q = __ldg(a.Wq + w);
-                    s = __ldg(a.Ws + w);
-                }
-            } else {
-                q = __ldg(qrow + (i - 1));
-                s = __ldg(srow + (i - 1));
+        const bool wall = (i == 0) || (i == nx - 1);
+        float q = 0.f, s = 0.f;
+        if (wall) {
+            // get_results_ writes 0 on a wall whose flux is not computed
+            if (i == 0 ? a.west : a.east) {
+                const long long w = (i == 0 ? 0LL : (long long)a.jmax * a.kloc) + wcell;
+                q = __ldg(a.Wq + w);
+                s = __ldg(a.Ws + w);
             }
-            const double T1 = __ldg(t1row + i);
-            double Qn = (double)q / a.stefan / a.Tin4;
-            if (wall) Qn = Qn / a.Height;
-            const double Vn = (double)s / a.stefan / a.Tin4;
-            const double x0 = T1 * a.Tin;
-            const double d = x0 - sT[0];
-            // t = int(x0 - x(1)) / int(x(2) - x(1)): both truncate toward zero
-            int t;
-            if (d > -2147483648.0 && d < 2147483648.0) t = (int)d / a.dT;
-            else t = (d > 0.0) ? a.nT : -1;  // far out of range, or NaN
-            if (t < 0 || t > a.nT - 2) {
-                ++clamped;
-                t = (t < 0) ? 0 : a.nT - 2;
-            }
-            const double K = sS[t] * (x0 - sT[t]) + sK[t];
-            Qn = Qn * a.underrelax;
-            const double t2 = T1 * T1;
-            const double G = 4.0 * (t2 * t2) - Qn / K;
-            a.Qnew[c] = Qn;
-            a.Varnew[c] = Vn;
-            a.Knew[c] = K;
-            a.Gnew[c] = G;
+        } else {
+            q = __ldg(a.Qc + (wcell * a.imax + (i - 1)));
+            s = __ldg(a.Sc + (wcell * a.imax + (i - 1)));
         }
+        const double T1 = __ldg(a.T1 + (i + (long long)nx * (jl + (long long)(a.jn + 2) * kl)));
+        double Qn = (double)q / a.stefan / a.Tin4;
+        if (wall) Qn = Qn / a.Height;
+        const double Vn = (double)s / a.stefan / a.Tin4;
+        const double x0 = T1 * a.Tin;
+        const double d = x0 - sT[0];
+        // t = int(x0 - x(1)) / int(x(2) - x(1)): both truncate toward zero
+        int t;
+        if (d > -2147483648.0 && d < 2147483648.0) {
+            const int ti = (int)d;
+            const int tq = (int)fdiv((unsigned long long)(ti < 0 ? -(long long)ti : ti), a.MdT);
+            t = ti < 0 ? -tq : tq;
+        } else {
+            t = (d > 0.0) ? a.nT : -1;  // far out of range, or NaN
+        }
+        if (t < 0 || t > a.nT - 2) {
+            ++clamped;
+            t = (t < 0) ? 0 : a.nT - 2;
+        }
+        const double K = sS[t] * (x0 - sT[t]) + sK[t];
+        Qn = Qn * a.underrelax;
+        const double t2 = T1 * T1;
+        const double G = 4.0 * (t2 * t2) - Qn / K;
+        a.Qnew[c] = Qn;
+        a.Varnew[c] = Vn;
+        a.Knew[c] = K;
+        a.Gnew[c] = G;
     }
     if (a.n_clamped) {
         const unsigned int w = __reduce_add_sync(0xffffffffu, clamped);
@@ -115,8 +118,9 @@ int dns_args(const rc_ctx *c, const rc_dns_coupling *cfg, DnsArgs &a, std::strin
         return set_err(err_, RC_E_INVALID, "coupling nTemp must be in 2..RC_DNS_MAX_T");
     if (cfg->jstart < 1 || cfg->jend > p.jmax || cfg->jstart > cfg->jend)
         return set_err(err_, RC_E_INVALID, "coupling j range outside 1..jmax");
-    if ((long long)(cfg->jend - cfg->jstart + 1) * c->kloc > 0x7fffffffLL)
-        return set_err(err_, RC_E_INVALID, "coupling pencil has more than 2^31 rows");
+    // fdiv(c, M) is exact when c * divisor < 2^64: c < cells, divisor <= imax+2
+    if ((long double)(p.imax + 2) * (cfg->jend - cfg->jstart + 1) * c->kloc * (p.imax + 2) >= 1.8e19L)
+        return set_err(err_, RC_E_INVALID, "coupling pencil too large");
     if (!(cfg->Tin > 0.0) || !std::isfinite(cfg->Tin) || cfg->stefan == 0.0 || cfg->Height == 0.0)
         return set_err(err_, RC_E_INVALID, "coupling needs Tin > 0 and non-zero stefan and Height");
     const double step = cfg->Tnb[1] - cfg->Tnb[0];
@@ -137,6 +141,9 @@ int dns_args(const rc_ctx *c, const rc_dns_coupling *cfg, DnsArgs &a, std::strin
     a.east = p.calcwalls && p.adiabe;
     a.nT = cfg->nTemp;
     a.dT = (int)step;
+    a.Mnx = Impl<float>::magic((unsigned long long)(p.imax + 2));
+    a.Mjn = Impl<float>::magic((unsigned long long)a.jn);
+    a.MdT = Impl<float>::magic((unsigned long long)a.dT);
     for (int t = 0; t < cfg->nTemp; ++t) {
         a.Tnb[t] = cfg->Tnb[t];
         a.kP[t] = cfg->kP[t];
@@ -155,9 +162,16 @@ SlotCommon *slot_of(rc_ctx *c, rc_ticket t) {
 }
 
 int launch_dns(const rc_ctx *c, const DnsArgs &a, cudaStream_t st, std::string *err_) {
-    const int rows = a.jn * a.kloc;
-    const int grid = std::max(1, std::min(rows, c->num_sms * 16));
-    k_dns_source<<<grid, 128, 0, st>>>(a);
+    // every block resident at once: the SMs' worth of blocks, at most one
+    // cell per thread
+    static int per_sm = 0;
+    if (!per_sm) {
+        RC_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_dns_source, 256, 0));
+        per_sm = std::max(per_sm, 1);
+    }
+    const long long n = (long long)(a.imax + 2) * a.jn * a.kloc;
+    const int grid = (int)std::max<long long>(1, std::min<long long>((n + 255) / 256, (long long)c->num_sms * per_sm));
+    k_dns_source<<<grid, 256, 0, st>>>(a);
     RC_CK(cudaGetLastError());
     return RC_OK;
 }
