@@ -40,8 +40,12 @@ struct DnsArgs {
 
 // One thread per output cell (grid-stride), i fastest, so every load and
 // store of a warp is contiguous; (i, j, k) and linear_int's row come from
-// exact multiply-high divisions (fdiv) instead of integer division.
-__global__ void __launch_bounds__(256) k_dns_source(const __grid_constant__ DnsArgs a) {
+// exact multiply-high divisions (fdiv) instead of integer division.  The
+// kernel is bound by instruction issue: the five IEEE double divisions the
+// Fortran's statement order requires take most of its ~245 instructions per
+// cell (measured on B200; 6 resident blocks per SM were 2-3% faster than 4,
+// two cells per thread no faster).
+__global__ void __launch_bounds__(256, 6) k_dns_source(const __grid_constant__ DnsArgs a) {
     __shared__ double sT[RC_DNS_MAX_T], sK[RC_DNS_MAX_T], sS[RC_DNS_MAX_T];
     for (int t = threadIdx.x; t < a.nT; t += blockDim.x) {
         sT[t] = a.Tnb[t];
