@@ -173,6 +173,11 @@ int rc_solve_device_async(rc_ctx *ctx, const float *T_dev, int zstart, rc_ticket
  * and variance of the mean), qw64/vw64 [2][kloc][jmax] (west, east). */
 int rc_collect(rc_ctx *ctx, rc_ticket ticket, float *Q, float *sigma,
                double *q64, double *var64, double *qw64, double *vw64);
+/* Wait for a ticket and copy its compact double results (layouts as in
+ * rc_collect) into the caller's device arrays (any may be NULL); the
+ * ticket is consumed.  For callers that gather results over NCCL. */
+int rc_collect_device(rc_ctx *ctx, rc_ticket ticket, double *q64_dev, double *var64_dev,
+                      double *qw64_dev, double *vw64_dev);
 /* Device-side results of the last collected/finished ticket (no copy):
  * pointers to the compact double arrays described above. */
 int rc_device_results(rc_ctx *ctx, rc_ticket ticket, const double **q64,

@@ -116,6 +116,7 @@ _SIGS = [
     ("rc_solve_async", _I, [_VP, _FP, _I, C.POINTER(C.c_int32)]),
     ("rc_solve_device_async", _I, [_VP, _VP, _I, C.POINTER(C.c_int32)]),
     ("rc_collect", _I, [_VP, C.c_int32, _FP, _FP, _DP, _DP, _DP, _DP]),
+    ("rc_collect_device", _I, [_VP, C.c_int32, _VP, _VP, _VP, _VP]),
     ("rc_device_results", _I, [_VP, C.c_int32, C.POINTER(_VP), C.POINTER(_VP), C.POINTER(_VP), C.POINTER(_VP)]),
     ("rc_solve_info_get", _I, [_VP, C.c_int32, C.POINTER(RcSolveInfo)]),
     ("rc_set_launch", _I, [_VP, _I, _I, _I, _I]),

@@ -260,6 +260,13 @@ class Solver:
         fp = lambda a: a.ctypes.data_as(C.POINTER(C.c_float))
         L.check(L.lib().rc_collect(self.ctx, ticket, fp(Q), fp(S), None, None, None, None), self.ctx)
 
+    def collect_device(self, ticket: int, q64_dev: int, var64_dev: int = 0, qw64_dev: int = 0, vw64_dev: int = 0):
+        """rc_collect_device: the compact double results into device arrays
+        (pointers; 0 skips one); the ticket is consumed."""
+        v = lambda x: C.c_void_p(x) if x else None
+        L.check(L.lib().rc_collect_device(self.ctx, ticket, v(q64_dev), v(var64_dev), v(qw64_dev), v(vw64_dev)),
+                self.ctx)
+
     def wait_device(self, ticket: int):
         q = C.c_void_p()
         L.check(L.lib().rc_device_results(self.ctx, ticket, C.byref(q), None, None, None), self.ctx)

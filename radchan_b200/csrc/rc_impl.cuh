@@ -1016,6 +1016,25 @@ struct Impl : ImplBase {
             }
     }
 
+    int collect_device(rc_ticket t, double *q64, double *var64, double *qw64, double *vw64) {
+        std::string *err_ = &c->err;
+        Slot<R> *sp = find_slot(t);
+        if (!sp) return set_err(err_, RC_E_STATE, "unknown or already collected ticket");
+        Slot<R> &s = *sp;
+        const rc_params &p = c->p;
+        const size_t ncf = (size_t)p.imax * p.jmax * c->kloc;
+        const size_t nwc = (size_t)2 * p.jmax * c->kloc;
+        if (q64) RC_CK(cudaMemcpyAsync(q64, s.d_q64, ncf * sizeof(double), cudaMemcpyDeviceToDevice, s.st));
+        if (var64) RC_CK(cudaMemcpyAsync(var64, s.d_var64, ncf * sizeof(double), cudaMemcpyDeviceToDevice, s.st));
+        if (qw64) RC_CK(cudaMemcpyAsync(qw64, s.d_qw64, nwc * sizeof(double), cudaMemcpyDeviceToDevice, s.st));
+        if (vw64) RC_CK(cudaMemcpyAsync(vw64, s.d_vw64, nwc * sizeof(double), cudaMemcpyDeviceToDevice, s.st));
+        RC_CK(cudaStreamSynchronize(s.st));
+        s.state = 0;
+        s.ticket = -1;
+        if (s.h_sc->status & 2) return set_err(err_, RC_E_RANGE, "temperature field contains non-finite values");
+        return RC_OK;
+    }
+
     int device_results(rc_ticket t, const double **q64, const double **var64, const double **qw64,
                        const double **vw64) {
         std::string *err_ = &c->err;

@@ -173,6 +173,12 @@ int rc_collect(rc_ctx *c, rc_ticket t, float *Q, float *sigma, double *q64, doub
     return with_impl(c, [&](auto &im) { return im.collect(t, Q, sigma, q64, var64, qw64, vw64); });
 }
 
+int rc_collect_device(rc_ctx *c, rc_ticket t, double *q64, double *var64, double *qw64, double *vw64) {
+    if (!c) return set_err(nullptr, RC_E_INVALID, "NULL context");
+    cudaSetDevice(c->device);
+    return with_impl(c, [&](auto &im) { return im.collect_device(t, q64, var64, qw64, vw64); });
+}
+
 int rc_device_results(rc_ctx *c, rc_ticket t, const double **q64, const double **var64, const double **qw64,
                       const double **vw64) {
     if (!c) return set_err(nullptr, RC_E_INVALID, "NULL context");
