@@ -19,6 +19,8 @@
 // slope*(x0-x(t)) + y(t).  Tin^4 is pow(Tin, 4.0) on the host, as Tin**4.
 // is in the DNS.  T1**4. is evaluated as (T1 T1)(T1 T1).
 #include <cmath>
+#include <thread>
+#include <vector>
 
 #include "rc_impl.cuh"
 
@@ -183,6 +185,27 @@ int launch_dns(const rc_ctx *c, const DnsArgs &a, cudaStream_t st, std::string *
 size_t pencil_cells(const DnsArgs &a) { return (size_t)(a.imax + 2) * (a.jn + 2) * (a.kloc + 2); }
 size_t out_cells(const DnsArgs &a) { return (size_t)(a.imax + 2) * a.jn * a.kloc; }
 
+// memcpy split over up to 8 host threads (parts of >= 4 MB): one thread
+// does not keep up with the PCIe copy engines.
+void par_copy(void *dst, const void *src, size_t bytes) {
+    const size_t min_part = (size_t)4 << 20;
+    const unsigned hw = std::max(1u, std::min(std::thread::hardware_concurrency(), 8u));
+    const size_t nt = std::max<size_t>(1, std::min<size_t>(hw, bytes / min_part));
+    if (nt <= 1) {
+        memcpy(dst, src, bytes);
+        return;
+    }
+    const size_t part = ((bytes + nt - 1) / nt + 63) & ~(size_t)63;
+    std::vector<std::thread> th;
+    for (size_t i = 1; i < nt; ++i) {
+        const size_t o = i * part;
+        if (o >= bytes) break;
+        th.emplace_back([=] { memcpy((char *)dst + o, (const char *)src + o, std::min(part, bytes - o)); });
+    }
+    memcpy(dst, src, std::min(part, bytes));
+    for (auto &x : th) x.join();
+}
+
 }  // namespace
 
 extern "C" {
@@ -207,6 +230,13 @@ int rc_dns_source(rc_ctx *c, rc_ticket t, const rc_dns_coupling *cfg, const doub
         RC_CK(cudaMalloc((void **)&c->d_dns, (np + 4 * no) * sizeof(double)));
         c->dns_cap = np + 4 * no;
     }
+    if (c->dns_hcap < np + 4 * no) {
+        if (c->h_dns) cudaFreeHost(c->h_dns);
+        c->h_dns = nullptr;
+        c->dns_hcap = 0;
+        RC_CK(cudaHostAlloc((void **)&c->h_dns, (np + 4 * no) * sizeof(double), cudaHostAllocDefault));
+        c->dns_hcap = np + 4 * no;
+    }
     if (!c->d_dns_n) RC_CK(cudaMalloc((void **)&c->d_dns_n, sizeof(unsigned long long)));
     double *dT1 = c->d_dns, *dQ = dT1 + np, *dV = dQ + no, *dK = dV + no, *dG = dK + no;
     a.Qc = s.d_Qc;
@@ -219,17 +249,35 @@ int rc_dns_source(rc_ctx *c, rc_ticket t, const rc_dns_coupling *cfg, const doub
     a.Knew = dK;
     a.Gnew = dG;
     a.n_clamped = c->d_dns_n;
+    // T1 through the pinned staging buffer (the field is staged while the
+    // solve may still run), then the kernel; each output array comes back
+    // into the staging buffer and is copied out while the next one is in
+    // flight
+    double *hT1 = c->h_dns, *hOut = c->h_dns + np;
+    par_copy(hT1, T1, np * sizeof(double));
     RC_CK(cudaEventSynchronize(s.e1));
     s.state = 2;
-    RC_CK(cudaMemcpyAsync(dT1, T1, np * sizeof(double), cudaMemcpyHostToDevice, s.st));
+    RC_CK(cudaMemcpyAsync(dT1, hT1, np * sizeof(double), cudaMemcpyHostToDevice, s.st));
     RC_CK(cudaMemsetAsync(c->d_dns_n, 0, sizeof(unsigned long long), s.st));
     rc = launch_dns(c, a, s.st, err_);
     if (rc) return rc;
+    cudaEvent_t ev[4] = {};
+    double *const dst[4] = {Qnew, Varnew, Knew, Gnew};
+    for (int q = 0; q < 4 && !rc; ++q) {
+        if (cudaEventCreateWithFlags(&ev[q], cudaEventDisableTiming) != cudaSuccess ||
+            cudaMemcpyAsync(hOut + q * no, dQ + q * no, no * sizeof(double), cudaMemcpyDeviceToHost, s.st) !=
+                cudaSuccess ||
+            cudaEventRecord(ev[q], s.st) != cudaSuccess)
+            rc = set_err(err_, RC_E_CUDA, "staging the DNS source terms failed");
+    }
+    for (int q = 0; q < 4 && !rc; ++q) {
+        if (cudaEventSynchronize(ev[q]) != cudaSuccess) rc = set_err(err_, RC_E_CUDA, "DNS source copy failed");
+        else par_copy(dst[q], hOut + q * no, no * sizeof(double));
+    }
+    for (auto &e : ev)
+        if (e) cudaEventDestroy(e);
+    if (rc) return rc;
     unsigned long long nc = 0;
-    RC_CK(cudaMemcpyAsync(Qnew, dQ, no * sizeof(double), cudaMemcpyDeviceToHost, s.st));
-    RC_CK(cudaMemcpyAsync(Varnew, dV, no * sizeof(double), cudaMemcpyDeviceToHost, s.st));
-    RC_CK(cudaMemcpyAsync(Knew, dK, no * sizeof(double), cudaMemcpyDeviceToHost, s.st));
-    RC_CK(cudaMemcpyAsync(Gnew, dG, no * sizeof(double), cudaMemcpyDeviceToHost, s.st));
     RC_CK(cudaMemcpyAsync(&nc, c->d_dns_n, sizeof(nc), cudaMemcpyDeviceToHost, s.st));
     RC_CK(cudaStreamSynchronize(s.st));
     if (n_clamped) *n_clamped = (long long)nc;

@@ -148,6 +148,8 @@ struct rc_ctx {
     double *d_dns = nullptr;
     size_t dns_cap = 0;
     unsigned long long *d_dns_n = nullptr;
+    double *h_dns = nullptr;  // pinned staging of the same arrays
+    size_t dns_hcap = 0;
     // precision-specific state
     void *impl = nullptr;  // Impl<float> or Impl<double>
     int dbl = 0;

@@ -236,6 +236,7 @@ int rc_destroy(rc_ctx *c) {
     }
     if (c->d_dns) cudaFree(c->d_dns);
     if (c->d_dns_n) cudaFree(c->d_dns_n);
+    if (c->h_dns) cudaFreeHost(c->h_dns);
     delete c;
     return RC_OK;
 }
