@@ -212,6 +212,7 @@ extern "C" {
 
 int rc_dns_source(rc_ctx *c, rc_ticket t, const rc_dns_coupling *cfg, const double *T1, double *Qnew, double *Varnew,
                   double *Knew, double *Gnew, long long *n_clamped) {
+    Range nv("rc_dns_source");
     if (!c) return set_err(nullptr, RC_E_INVALID, "NULL context");
     std::string *err_ = &c->err;
     if (!T1 || !Qnew || !Varnew || !Knew || !Gnew) return set_err(err_, RC_E_INVALID, "NULL array");

@@ -20,6 +20,8 @@
 #include <string>
 #include <vector>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "rc_host.h"
 #include "rc_kernels.cuh"
 
@@ -36,6 +38,16 @@ inline int set_err(std::string *dst, int code, const std::string &m) {
     g_err = m;
     return code;
 }
+
+// NVTX range over a host scope (solve enqueue, collect, batch, server
+// quantum, DNS coupling): a profiler shows the kernels each one launched
+// under its name; without a profiler attached the calls do nothing.
+struct Range {
+    explicit Range(const char *name) { nvtxRangePushA(name); }
+    ~Range() { nvtxRangePop(); }
+    Range(const Range &) = delete;
+    Range &operator=(const Range &) = delete;
+};
 }  // namespace rc_detail
 
 #define RC_CK(call)                                                                                    \
@@ -838,6 +850,7 @@ struct Impl : ImplBase {
     }
 
     int solve(const float *T, bool device_ptr, int zstart, rc_ticket *ticket) {
+        Range nv("rc_solve");
         std::string *err_ = &c->err;
         int rc = check_solve_args(T, zstart);
         if (rc) return rc;
@@ -898,6 +911,7 @@ struct Impl : ImplBase {
     }
 
     int autotune(const float *T, int zstart, int pilot, int *rpt_out, int *block_out, int *sort_out, int *occ_out) {
+        Range nv("rc_autotune");
         std::string *err_ = &c->err;
         int rc = check_solve_args(T, zstart);
         if (rc) return rc;
@@ -957,6 +971,7 @@ struct Impl : ImplBase {
     }
 
     int collect(rc_ticket t, float *Q, float *sigma, double *q64, double *var64, double *qw64, double *vw64) {
+        Range nv("rc_collect");
         std::string *err_ = &c->err;
         Slot<R> *sp = find_slot(t);
         if (!sp) return set_err(err_, RC_E_STATE, "unknown or already collected ticket");
@@ -1019,6 +1034,7 @@ struct Impl : ImplBase {
     }
 
     int collect_device(rc_ticket t, double *q64, double *var64, double *qw64, double *vw64) {
+        Range nv("rc_collect_device");
         std::string *err_ = &c->err;
         Slot<R> *sp = find_slot(t);
         if (!sp) return set_err(err_, RC_E_STATE, "unknown or already collected ticket");

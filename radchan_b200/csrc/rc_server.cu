@@ -348,6 +348,7 @@ int start_stage(rc_server *sv, SrvReq *r, cudaStream_t st) {
 // marching request's remaining tiles in one persistent launch.  Set-up work
 // of new stages was enqueued on the same stream just before.
 int run_quantum(rc_server *sv, const std::vector<SrvReq *> &marching, int par) {
+    Range nv("rc_server quantum");
     std::string *err_ = &sv->err;
     const int n = (int)marching.size();
     cudaStream_t st = sv->qst[par];
@@ -414,6 +415,7 @@ int run_quantum(rc_server *sv, const std::vector<SrvReq *> &marching, int par) {
 // Tallies of the requests whose last tiles were just issued, on the tally
 // stream after every quantum in flight (any of them may hold their tiles).
 int enqueue_tallies(rc_server *sv, const std::vector<SrvReq *> &marching) {
+    Range nv("rc_server tallies");
     std::string *err_ = &sv->err;
     bool waited = false;
     for (SrvReq *r : marching) {

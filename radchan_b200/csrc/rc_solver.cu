@@ -425,6 +425,7 @@ int rc_batch_add(rc_batch *b, rc_ctx *c, const float *T_host, int zstart) {
 }
 
 int rc_batch_run(rc_batch *b) {
+    Range nv("rc_batch_run");
     if (!b) return set_err(nullptr, RC_E_INVALID, "NULL batch");
     if (b->m.empty()) return set_err(&b->err, RC_E_STATE, "empty batch");
     cudaSetDevice(b->device);
@@ -470,6 +471,7 @@ int rc_batch_run(rc_batch *b) {
 }
 
 int rc_batch_wait(rc_batch *b, float *ms_device) {
+    Range nv("rc_batch_wait");
     if (!b) return set_err(nullptr, RC_E_INVALID, "NULL batch");
     cudaSetDevice(b->device);
     std::string *err_ = &b->err;
