@@ -155,6 +155,12 @@ int rc_tables_synthetic(const rc_synth_spec *spec, rc_table_set **out);
  * dir in the formats of nbcorrk/write_tables.cpp:23-107. */
 int rc_tables_read_dir(const char *dir, int nT, int nB, int nQ, rc_table_set **out);
 int rc_tables_write_dir(const rc_table_set *ts, const char *dir);
+/* Check what the solver assumes of a table set (rc_set_tables runs the same
+ * check): 2..256 increasing, uniformly spaced temperatures; cumulative
+ * probabilities finite, non-decreasing and within [0, 1]; absorption and
+ * Planck-mean coefficients finite and >= 0.  RC_E_INVALID with the first
+ * violation in msg otherwise.  Needs no GPU. */
+int rc_tables_validate(const rc_tables *t, char *msg, size_t msglen);
 /* Borrowed view of a table set (valid until rc_tables_free). */
 int rc_tables_view(const rc_table_set *ts, rc_tables *view);
 void rc_tables_free(rc_table_set *ts);

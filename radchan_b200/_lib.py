@@ -110,6 +110,7 @@ _SIGS = [
     ("rc_tables_read_dir", _I, [C.c_char_p, _I, _I, _I, C.POINTER(_VP)]),
     ("rc_tables_write_dir", _I, [_VP, C.c_char_p]),
     ("rc_tables_view", _I, [_VP, C.POINTER(RcTables)]),
+    ("rc_tables_validate", _I, [C.POINTER(RcTables), C.c_char_p, C.c_size_t]),
     ("rc_tables_free", None, [_VP]),
     ("rc_create", _I, [C.POINTER(RcParams), _I, C.POINTER(_VP)]),
     ("rc_set_tables", _I, [_VP, C.POINTER(RcTables)]),

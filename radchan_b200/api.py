@@ -86,6 +86,13 @@ class TableSet:
     def write_dir(self, path):
         L.check(L.lib().rc_tables_write_dir(self.h, str(path).encode()))
 
+    def validate(self) -> str:
+        """rc_tables_validate: "" when the set meets the solver's
+        assumptions, else the first violation."""
+        buf = C.create_string_buffer(512)
+        rc = L.lib().rc_tables_validate(C.byref(self.view), buf, 512)
+        return "" if rc == L.RC_OK else buf.value.decode(errors="replace")
+
     def arrays(self):
         v = self.view
         nT, nB, nQ = v.nT, v.nB, v.nQ

@@ -836,6 +836,44 @@ int tables_synthetic(const rc_synth_spec &s, TableSet &t, std::string &err) {
     return RC_OK;
 }
 
+int tables_check(const TableSet &t, std::string &err) {
+    auto bad = [&](const std::string &m) {
+        err = m;
+        return RC_E_INVALID;
+    };
+    if (t.nT < 2 || t.nB < 1 || t.nQ < 1) return bad("table dimensions must be nT >= 2, nB >= 1, nQ >= 1");
+    if (t.nT > 256) return bad("at most 256 table temperatures");
+    const size_t nT = t.nT, nB = t.nB, nQ = t.nQ;
+    if (t.Tnb.size() < nT || t.kP.size() < nT || t.kq.size() < nB * nT * nQ || t.prob.size() < nT * nB ||
+        t.probg.size() < nT * nB * nQ)
+        return bad("table arrays shorter than their dimensions");
+    if (!(t.Tnb[1] > t.Tnb[0]) || !std::isfinite(t.Tnb[0]) || !std::isfinite(t.Tnb[1]))
+        return bad("table temperatures must be increasing");
+    const double d0 = (double)t.Tnb[1] - t.Tnb[0];
+    for (size_t i = 2; i < nT; ++i) {
+        // the lookups assume uniform spacing (pos = (T - T0)/dT)
+        const double di = (double)t.Tnb[i] - t.Tnb[i - 1];
+        if (!(fabs(di - d0) <= 1e-3 * fabs(d0))) return bad("table temperatures must be uniformly spaced");
+    }
+    // the band and g searches assume non-decreasing cumulative
+    // probabilities in [0, 1] (a NaN fails every comparison below)
+    const float one = 1.0f + 1e-5f;
+    for (size_t i = 0; i < nT; ++i) {
+        for (size_t b = 0; b < nB; ++b) {
+            const float v = t.prob[i * nB + b], prev = b ? t.prob[i * nB + b - 1] : 0.0f;
+            if (!(v >= prev && v <= one)) return bad("band cumulative probability not non-decreasing in [0, 1] (prob_new2)");
+            for (size_t g = 0; g < nQ; ++g) {
+                const float u = t.probg[(i * nB + b) * nQ + g], pu = g ? t.probg[(i * nB + b) * nQ + g - 1] : 0.0f;
+                if (!(u >= pu && u <= one)) return bad("g cumulative probability not non-decreasing in [0, 1] (prob_new2)");
+            }
+        }
+        if (!(t.kP[i] >= 0.0f) || !std::isfinite(t.kP[i])) return bad("Planck-mean coefficient not finite and >= 0");
+    }
+    for (size_t q = 0; q < nB * nT * nQ; ++q)
+        if (!(t.kq[q] >= 0.0f) || !std::isfinite(t.kq[q])) return bad("absorption coefficient not finite and >= 0 (NarrBand)");
+    return RC_OK;
+}
+
 namespace {
 bool read_numbers(const std::string &path, std::vector<double> &v) {
     FILE *f = fopen(path.c_str(), "r");

@@ -47,6 +47,12 @@ struct TableSet {
 int tables_synthetic(const rc_synth_spec &s, TableSet &out, std::string &err);
 int tables_read_dir(const std::string &dir, int nT, int nB, int nQ, TableSet &out, std::string &err);
 int tables_write_dir(const TableSet &ts, const std::string &dir, std::string &err);
+// What the device lookups assume of a table set: 2..256 increasing,
+// uniformly spaced temperatures; cumulative probabilities finite,
+// non-decreasing, within [0, 1]; absorption coefficients and the
+// Planck-mean coefficient finite and >= 0.  RC_E_INVALID and a message
+// naming the first violation otherwise.
+int tables_check(const TableSet &t, std::string &err);
 
 // Gauss-Legendre nodes/weights on [-1, 1] (Newton iteration on P_n).
 void gauss_legendre(int n, std::vector<double> &x, std::vector<double> &w);

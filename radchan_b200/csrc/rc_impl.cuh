@@ -478,24 +478,9 @@ struct Impl : ImplBase {
         if (p.grey) return set_err(err_, RC_E_INVALID, "grey mode builds its own tables; rc_set_tables not used");
         if (t.nT != p.nT || t.nB != p.nB || t.nQ != p.nQ)
             return set_err(err_, RC_E_INVALID, "table dimensions differ from params nT/nB/nQ");
-        if (t.nT < 2 || !(t.Tnb[1] > t.Tnb[0]))
-            return set_err(err_, RC_E_INVALID, "table temperatures must be increasing");
-        if (t.nT > 256) return set_err(err_, RC_E_INVALID, "at most 256 table temperatures");
-        for (int i = 0; i < t.nT; ++i) {
-            // the band search assumes non-decreasing cumulative probabilities
-            for (int b = 1; b < t.nB; ++b)
-                if (t.prob[(size_t)i * t.nB + b] < t.prob[(size_t)i * t.nB + b - 1])
-                    return set_err(err_, RC_E_INVALID, "band cumulative probability decreases (prob_new2)");
-            for (int b = 0; b < t.nB; ++b)
-                for (int g = 1; g < t.nQ; ++g)
-                    if (t.probg[((size_t)i * t.nB + b) * t.nQ + g] < t.probg[((size_t)i * t.nB + b) * t.nQ + g - 1])
-                        return set_err(err_, RC_E_INVALID, "g cumulative probability decreases (prob_new2)");
-        }
-        for (int i = 2; i < t.nT; ++i) {
-            // the lookups assume uniform spacing (pos = (T - T0)/dT)
-            const double d0 = t.Tnb[1] - t.Tnb[0], di = t.Tnb[i] - t.Tnb[i - 1];
-            if (fabs(di - d0) > 1e-3 * fabs(d0))
-                return set_err(err_, RC_E_INVALID, "table temperatures must be uniformly spaced");
+        {
+            std::string m;
+            if (tables_check(t, m)) return set_err(err_, RC_E_INVALID, m);
         }
         release_tables();
         nT = t.nT;

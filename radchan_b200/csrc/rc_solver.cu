@@ -70,6 +70,17 @@ int rc_tables_write_dir(const rc_table_set *ts, const char *dir) {
     return RC_OK;
 }
 
+int rc_tables_validate(const rc_tables *t, char *msg, size_t msglen) {
+    if (!t) return set_err(nullptr, RC_E_INVALID, "NULL tables");
+    TableSet ts;
+    ts.from_view(t);
+    std::string err;
+    const int rc = tables_check(ts, err);
+    if (msg && msglen) snprintf(msg, msglen, "%s", err.c_str());
+    if (rc) return set_err(nullptr, rc, err);
+    return RC_OK;
+}
+
 int rc_tables_view(const rc_table_set *ts, rc_tables *view) {
     if (!ts || !view) return set_err(nullptr, RC_E_INVALID, "NULL argument");
     ts->ts.view(view);

@@ -119,6 +119,47 @@ def test_reference_table_files_round_trip(tmp_path):
     assert len(lines[0].split()) == 3 + 8
 
 
+def _edit_token(path, line, col, value):
+    lines = open(path).read().split("\n")
+    tok = lines[line].split()
+    tok[col] = value
+    lines[line] = " ".join(tok)
+    open(path, "w").write("\n".join(lines))
+
+
+@pytest.mark.parametrize("fname,line,col,value,msg", [
+    ("prob_new2.txt", 3, 2, "1.0e-3", "band cumulative"),      # band CDF decreases
+    ("prob_new2.txt", 2, 4, "nan", "g cumulative"),             # NaN in a g CDF
+    ("prob_new2.txt", 1, 6, "1.5", "g cumulative"),             # g CDF above 1
+    ("NarrBand3.txt", 2, 4, "-2.0e-03", "absorption"),          # negative k
+    ("NarrBand1.txt", 4, 3, "inf", "absorption"),               # infinite k
+    ("planck-mean.txt", 2, 0, "1200.0", "uniformly"),           # uneven temperature step
+    ("planck-mean.txt", 3, 1, "nan", "Planck-mean"),            # NaN kP
+])
+def test_malformed_table_files_are_rejected(tmp_path, fname, line, col, value, msg):
+    """Table files that read but break what the device searches assume
+    (monotone CDFs in [0, 1], finite k >= 0, uniform temperature steps)
+    are rejected before any upload, with the first violation named."""
+    ts = W.tables_nb(nB=6, nQ=4, nT=5)
+    assert ts.validate() == ""
+    ts.write_dir(tmp_path)
+    assert api.TableSet.read_dir(tmp_path, 5, 6, 4).validate() == ""
+    _edit_token(os.path.join(tmp_path, fname), line, col, value)
+    bad = api.TableSet.read_dir(tmp_path, 5, 6, 4)
+    assert msg in bad.validate()
+
+
+def test_truncated_table_file_is_reported(tmp_path):
+    ts = W.tables_nb(nB=6, nQ=4, nT=5)
+    ts.write_dir(tmp_path)
+    path = os.path.join(tmp_path, "prob_new2.txt")
+    text = open(path).read()
+    open(path, "w").write(text[: len(text) // 2])
+    with pytest.raises(Exception) as e:
+        api.TableSet.read_dir(tmp_path, 5, 6, 4)
+    assert "prob_new2" in str(e.value)
+
+
 def test_missing_table_file_is_reported(tmp_path):
     with pytest.raises(Exception) as e:
         api.TableSet.read_dir(tmp_path, 16, 12, 8)
