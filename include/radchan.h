@@ -56,6 +56,7 @@ extern "C" {
 #define RC_E_RANGE      -6   /* T outside the table range or not finite */
 #define RC_E_BUSY       -7   /* no free slot / queue full */
 #define RC_E_NOTFOUND   -8
+#define RC_E_CANCELLED  -9   /* a served request was cancelled */
 
 /* wall indices: west (x=0), east (x=Lx), south (y=0), north (y=Ly),
  * bottom (z=0), top (z=Lz) -- the order of param.h:68-100 */
@@ -239,6 +240,15 @@ int rc_solve_noalloc(rc_ctx *ctx, const float *T_dev, int zstart, double *q64_de
                      double *qw64_dev, double *vw64_dev);
 int rc_destroy(rc_ctx *ctx);
 int rc_last_error(const rc_ctx *ctx, char *buf, size_t len);
+/* Failure injection for tests of the error paths (no counterpart in the
+ * reference): the next `count` times the named host-side site is reached
+ * (in any context or server of the process) it fails with RC_E_CUDA and
+ * the message "injected failure at <site>", without making its CUDA call,
+ * so no device fault is involved.  count 0 disarms.  Sites: "field_copy"
+ * (a solve's field copy and set-up), "march" and "tally" (their launches),
+ * "collect" (result copies), "dns" (the DNS coupling launch), "quantum"
+ * (a server march launch). */
+int rc_debug_fail_next(const char *site, int count);
 /* Grid faces/centres of level `level` as built by the library
  * (definitions.h:68-136); any pointer may be NULL. */
 int rc_grid_level(const rc_params *p, int level, float *xu, float *yu, float *zu,
@@ -311,6 +321,12 @@ int rc_server_quanta(rc_server *s, long long *quanta);
 #define RC_SCHED_FAIR 0
 #define RC_SCHED_SRPT 1
 int rc_server_set_policy(rc_server *s, int policy);
+/* Cancel a request: a queued one is dropped at once; a running one stops
+ * after the quanta in flight finish and its context returns to the pool.
+ * rc_server_wait then returns RC_E_CANCELLED (or the result, if the solve
+ * completed first).  RC_E_STATE if its result is already published,
+ * RC_E_NOTFOUND for an unknown (or already waited) id. */
+int rc_server_cancel(rc_server *s, int64_t id);
 int rc_server_destroy(rc_server *s);
 
 /* ---------------- DNS coupling ---------------- */

@@ -14,7 +14,7 @@ LIB_PATH = os.path.join(HERE, "libradchan.so")
 RC_MAX_LEVELS = 9
 RC_OK = 0
 RC_E = {-1: "RC_E_INVALID", -2: "RC_E_CUDA", -3: "RC_E_NOMEM", -4: "RC_E_IO", -5: "RC_E_STATE",
-        -6: "RC_E_RANGE", -7: "RC_E_BUSY", -8: "RC_E_NOTFOUND"}
+        -6: "RC_E_RANGE", -7: "RC_E_BUSY", -8: "RC_E_NOTFOUND", -9: "RC_E_CANCELLED"}
 RC_WEST, RC_EAST, RC_SOUTH, RC_NORTH, RC_BOT, RC_TOP = range(6)
 
 
@@ -127,6 +127,7 @@ _SIGS = [
     ("rc_solve_noalloc", _I, [_VP, _VP, _I, _VP, _VP, _VP, _VP]),
     ("rc_destroy", _I, [_VP]),
     ("rc_last_error", _I, [_VP, C.c_char_p, C.c_size_t]),
+    ("rc_debug_fail_next", _I, [C.c_char_p, _I]),
     ("rc_grid_level", _I, [C.POINTER(RcParams), _I, _FP, _FP, _FP, _FP, _FP, _FP]),
     ("rc_trace", _I, [_VP, C.c_int32, _I, C.POINTER(RcBundleId), C.POINTER(RcTraceRec), _I, C.POINTER(C.c_int)]),
     ("rc_batch_create", _I, [_I, _I, C.POINTER(_VP)]),
@@ -144,6 +145,7 @@ _SIGS = [
     ("rc_server_set_quantum", _I, [_VP, C.c_longlong]),
     ("rc_server_quanta", _I, [_VP, C.POINTER(C.c_longlong)]),
     ("rc_server_set_policy", _I, [_VP, _I]),
+    ("rc_server_cancel", _I, [_VP, C.c_int64]),
     ("rc_dns_source", _I, [_VP, C.c_int32, C.POINTER(RcDnsCoupling), _DP, _DP, _DP, _DP, _DP,
                            C.POINTER(C.c_longlong)]),
     ("rc_dns_source_device", _I, [_VP, C.c_int32, C.POINTER(RcDnsCoupling), _VP, _VP, _VP, _VP, _VP, _VP, _VP]),

@@ -452,6 +452,11 @@ class Server:
         L.check(L.lib().rc_server_wait(self.h, rid, fp(Q), fp(S), C.byref(info)))
         return ServedResult(Q, S, info.t_submit, info.t_admit, info.t_done, info.photmax, info.rel_std_maxq)
 
+    def cancel(self, rid: int):
+        """rc_server_cancel: wait(rid) then raises RC_E_CANCELLED, unless
+        the solve completed first."""
+        L.check(L.lib().rc_server_cancel(self.h, int(rid)))
+
     def set_quantum(self, tiles: int):
         L.check(L.lib().rc_server_set_quantum(self.h, int(tiles)))
 

@@ -168,6 +168,7 @@ SlotCommon *slot_of(rc_ctx *c, rc_ticket t) {
 }
 
 int launch_dns(const rc_ctx *c, const DnsArgs &a, cudaStream_t st, std::string *err_) {
+    RC_FAILPOINT("dns");
     // every block resident at once: the SMs' worth of blocks, at most one
     // cell per thread
     static int per_sm = 0;

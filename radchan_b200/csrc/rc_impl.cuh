@@ -14,7 +14,9 @@
 #include <string.h>
 
 #include <algorithm>
+#include <atomic>
 #include <chrono>
+#include <map>
 #include <memory>
 #include <mutex>
 #include <string>
@@ -39,6 +41,32 @@ inline int set_err(std::string *dst, int code, const std::string &m) {
     return code;
 }
 
+// Host-side failure injection (rc_debug_fail_next): a named site reached
+// while armed fails as if its CUDA call had returned an error, without
+// making the call, so error paths and recovery are tested with no device
+// fault.  Sites: field_copy, march, tally, collect, dns, quantum.
+struct FailPoints {
+    std::atomic<int> armed{0};
+    std::mutex mu;
+    std::map<std::string, int> left;
+};
+inline FailPoints &fail_points() {
+    static FailPoints f;
+    return f;
+}
+inline bool fail_now(const char *site) {
+    FailPoints &f = fail_points();
+    if (!f.armed.load(std::memory_order_relaxed)) return false;
+    std::lock_guard<std::mutex> lk(f.mu);
+    auto it = f.left.find(site);
+    if (it == f.left.end() || it->second <= 0) return false;
+    if (--it->second == 0) {
+        f.left.erase(it);
+        f.armed.fetch_sub(1);
+    }
+    return true;
+}
+
 // NVTX range over a host scope (solve enqueue, collect, batch, server
 // quantum, DNS coupling): a profiler shows the kernels each one launched
 // under its name; without a profiler attached the calls do nothing.
@@ -55,6 +83,11 @@ struct Range {
         cudaError_t e_ = (call);                                                                       \
         if (e_ != cudaSuccess)                                                                         \
             return set_err(err_, RC_E_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_));      \
+    } while (0)
+
+#define RC_FAILPOINT(site)                                                                             \
+    do {                                                                                               \
+        if (fail_now(site)) return set_err(err_, RC_E_CUDA, std::string("injected failure at ") + site); \
     } while (0)
 
 // ---------------------------------------------------------------------------
@@ -732,6 +765,7 @@ struct Impl : ImplBase {
     int launch_march(const DSolve<R> *d_solves, const long long *d_tiles, int nsolves, long long total_tiles,
                      unsigned long long *d_counter, int block, int rpt_max, cudaStream_t st, int minb = 0) {
         std::string *err_ = &c->err;
+        RC_FAILPOINT("march");
         if (minb <= 0) minb = c->minb;
         auto fn = march_fn(minb);
         const size_t smem = march_smem(block, rpt_max);
@@ -792,6 +826,7 @@ struct Impl : ImplBase {
     int prepare(Slot<R> &s, const float *T_dev, int zstart, int rpt, cudaStream_t st) {
         std::string *err_ = &c->err;
         const rc_params &p = c->p;
+        RC_FAILPOINT("field_copy");
         int rc = ensure_partial(s, rpt);
         if (rc) return rc;
         const size_t nfield = (size_t)(p.imax + 2) * (p.jmax + 2) * (p.kmax + 2);
@@ -823,6 +858,7 @@ struct Impl : ImplBase {
     int launch_tally(const DSolve<R> *d_solves, const TallyOut *d_outs, int nsolves, long long max_cells,
                      cudaStream_t st) {
         std::string *err_ = &c->err;
+        RC_FAILPOINT("tally");
         const int gt = (int)std::max<long long>(1, std::min<long long>((max_cells + 255) / 256, (long long)c->num_sms * 8));
         k_tally_multi<R><<<dim3(gt, nsolves), 256, 0, st>>>(d_solves, d_outs);
         RC_CK(cudaGetLastError());
@@ -973,6 +1009,7 @@ struct Impl : ImplBase {
     int copy_out(Slot<R> &s, float *Q, float *sigma, double *q64, double *var64, double *qw64, double *vw64) {
         std::string *err_ = &c->err;
         const rc_params &p = c->p;
+        RC_FAILPOINT("collect");
         const size_t ncf = (size_t)p.imax * p.jmax * c->kloc;
         const size_t nwc = (size_t)2 * p.jmax * c->kloc;
         if (Q || sigma) {

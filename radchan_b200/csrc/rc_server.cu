@@ -62,6 +62,7 @@ struct SrvReq {
     int stage = ST_QUEUED;
     int phase = PH_PREPARE;
     bool published = false;  // result visible to rc_server_wait (guarded by the server mutex)
+    bool cancel = false;     // rc_server_cancel on a running request (guarded by the server mutex)
     double t_submit = 0, t_admit = 0, t_done = 0;
     rc_ctx *ctx = nullptr;
     Slot<float> *slot = nullptr;
@@ -350,6 +351,7 @@ int start_stage(rc_server *sv, SrvReq *r, cudaStream_t st) {
 int run_quantum(rc_server *sv, const std::vector<SrvReq *> &marching, int par) {
     Range nv("rc_server quantum");
     std::string *err_ = &sv->err;
+    RC_FAILPOINT("quantum");
     const int n = (int)marching.size();
     cudaStream_t st = sv->qst[par];
     long long *ht = sv->h_tiles[par], *hb = sv->h_base[par];
@@ -535,6 +537,24 @@ void worker_loop(rc_server *sv) {
             if (sv->stop) break;
         }
         admit(sv);
+        // cancelled running requests: once no quantum or tally in flight
+        // can still touch their slots, they end and give their contexts back
+        {
+            std::vector<SrvReq *> cancelled;
+            {
+                std::lock_guard<std::mutex> lk(sv->mu);
+                for (SrvReq *r : sv->running)
+                    if (r->cancel && r->stage < ST_DONE) cancelled.push_back(r);
+            }
+            if (!cancelled.empty()) {
+                for (int q = 0; q < rc_server::kNQ; ++q) cudaStreamSynchronize(sv->qst[q]);
+                cudaStreamSynchronize(sv->st);
+                for (SrvReq *r : cancelled) {
+                    if (r->slot) cudaStreamSynchronize(r->slot->st);
+                    fail(sv, r, RC_E_CANCELLED, "request cancelled");
+                }
+            }
+        }
         const int par = sv->q_par;
         // at most kNQ quanta in flight: this parity's previous quantum must
         // have finished before its stream and buffers take the next one
@@ -734,6 +754,30 @@ int rc_server_wait(rc_server *sv, int64_t id, float *Q, float *sigma, rc_result_
     if (r->ev) cudaEventDestroy(r->ev);
     sv->reqs.erase(it);
     if (st) return set_err(nullptr, st, m);
+    return RC_OK;
+}
+
+int rc_server_cancel(rc_server *sv, int64_t id) {
+    if (!sv) return set_err(nullptr, RC_E_INVALID, "NULL server");
+    std::lock_guard<std::mutex> lk(sv->mu);
+    auto it = sv->reqs.find(id);
+    if (it == sv->reqs.end()) return set_err(nullptr, RC_E_NOTFOUND, "unknown request id");
+    SrvReq *r = it->second.get();
+    if (r->published) return set_err(nullptr, RC_E_STATE, "request already finished");
+    for (auto q = sv->queue.begin(); q != sv->queue.end(); ++q)
+        if (*q == r) {
+            // not admitted: nothing of it is on the device
+            sv->queue.erase(q);
+            r->status = RC_E_CANCELLED;
+            r->err = "request cancelled";
+            r->stage = ST_FAILED;
+            r->t_done = now_s();
+            r->published = true;
+            sv->cv_done.notify_all();
+            return RC_OK;
+        }
+    r->cancel = true;
+    sv->cv_work.notify_all();
     return RC_OK;
 }
 

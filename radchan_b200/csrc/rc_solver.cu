@@ -258,6 +258,28 @@ int rc_last_error(const rc_ctx *c, char *buf, size_t len) {
     return RC_OK;
 }
 
+int rc_debug_fail_next(const char *site, int count) {
+    static const char *const sites[] = {"field_copy", "march", "tally", "collect", "dns", "quantum"};
+    if (!site || count < 0) return set_err(nullptr, RC_E_INVALID, "NULL site or negative count");
+    bool known = false;
+    for (const char *s : sites) known = known || strcmp(s, site) == 0;
+    if (!known) return set_err(nullptr, RC_E_INVALID, std::string("unknown failure site ") + site);
+    FailPoints &f = fail_points();
+    std::lock_guard<std::mutex> lk(f.mu);
+    auto it = f.left.find(site);
+    const bool was = it != f.left.end();
+    if (count == 0) {
+        if (was) {
+            f.left.erase(it);
+            f.armed.fetch_sub(1);
+        }
+    } else {
+        f.left[site] = count;
+        if (!was) f.armed.fetch_add(1);
+    }
+    return RC_OK;
+}
+
 }  // extern "C"
 
 // ---------------------------------------------------------------------------
