@@ -195,7 +195,9 @@ typedef struct rc_solve_info {
     float kappamax;        /* Planck-mean k at Tmax */
     float Ibmax_fluid;     /* energy per fluid bundle */
     int   table_row;       /* table row nearest Tmax (mc_gpu_noint.cu:1110) */
-    int   status;          /* bit 0: T outside table range, bit 1: non-finite T */
+    int   status;          /* bit 0: T outside table range, bit 1: non-finite T;
+                              bounds-checked build (libradchan_checked.so): bit 3 an
+                              index was out of bounds, bits 8-15 the first such site */
     double bundles;        /* bundles traced */
     double steps;          /* ray-cell steps */
     float ms_device;       /* device time of the march kernel */

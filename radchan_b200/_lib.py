@@ -9,7 +9,9 @@ import ctypes as C
 import os
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "libradchan.so")
+# RADCHAN_LIB=checked loads the bounds-checked build (libradchan_checked.so)
+LIB_PATH = os.path.join(HERE, "libradchan_checked.so" if os.environ.get("RADCHAN_LIB") == "checked"
+                        else "libradchan.so")
 
 RC_MAX_LEVELS = 9
 RC_OK = 0

@@ -67,9 +67,9 @@ struct alignas(4 * sizeof(R)) KIRow {
 struct DScalars {
     unsigned int tmax_bits;   // float bits of max T (non-negative)
     unsigned int tmin_bits;   // float bits of min T
-    int status;               // bit 0 out of table, bit 1 non-finite, bit 2 T <= 0
+    int status;               // bit 0 out of table, bit 1 non-finite, bit 2 T <= 0, bit 3 index out of bounds
     int tm, row;
-    int pad;
+    int bad_site;             // first out-of-bounds site (bounds-checked build)
     double Tmax, kappamax, Ibmax_f, Ibmax_w[2];
     double T0, inv_dT;        // first table temperature and 1/spacing
     int Pm;                   // table coordinate of Tmax
@@ -121,7 +121,35 @@ struct DSolve {
     unsigned long long nwc;   // jmax * kloc
     uint32_t key0, key1;
     long long tile_base;      // first tile of this launch within the solve (server quanta)
+    // extents for the bounds-checked build
+    long long n_faces, n_P, n_partial;
 };
+
+// Bounds-checked indexing.  The product build compiles RC_IX to the plain
+// index.  A build with RC_CHECKED=1 (libradchan_checked.so) checks every
+// table, field and partial-sum index of the march against its array's
+// extent: an index outside [0, n) sets status bit 3 and the first offending
+// site in DScalars::bad_site, and is replaced by 0 so the access stays
+// inside the array.  Nothing traps.
+#ifndef RC_CHECKED
+#define RC_CHECKED 0
+#endif
+enum RcSite : int {
+    SITE_FACE = 1, SITE_PYRAMID, SITE_ROW, SITE_IBW, SITE_WALL_T, SITE_WALL_ROW, SITE_CENTRE, SITE_EMIT_T,
+    SITE_WALL_EMIT_T, SITE_FACE_SHIFT, SITE_EMIT_ROW, SITE_DEN, SITE_IBM, SITE_PROBG, SITE_PARTIAL, SITE_LEVEL,
+    SITE_CDF
+};
+#if RC_CHECKED
+__device__ __forceinline__ long long rc_ix(long long i, long long n, int site, DScalars *sc) {
+    if (i >= 0 && i < n) return i;
+    atomicOr(&sc->status, 8);
+    atomicCAS(&sc->bad_site, 0, site);
+    return 0;
+}
+#define RC_IX(i, n, site, S) rc_ix((long long)(i), (long long)(n), (site), (S).sc)
+#else
+#define RC_IX(i, n, site, S) (i)
+#endif
 
 // ---------------------------------------------------------------------------
 // precision traits
@@ -291,18 +319,22 @@ __device__ __forceinline__ bool emit_bundle(Emitted<R> &e, const DSolve<R> &S, i
     int Pi;
     int nb, g, ic = i;
     R st;
-    e.yp = S.yc[j];
-    e.zp = S.zc[k];
+    e.yp = S.yc[RC_IX(j, S.jmax + 2, SITE_CENTRE, S)];
+    e.zp = S.zc[RC_IX(k, S.kmax + 2, SITE_CENTRE, S)];
     if (kind == 0) {
         // isotropic: cos(theta) = 1 - 2u (emiss_ang, :1077-1084)
         const R mu = (R)1 - (R)2 * u_mu;
         st = RT<R>::sqrt_(((R)1 - mu) * ((R)1 + mu));
         e.sx = mu;
-        nb = guided_index(S.cdf_f, S.guide_f, S.nB, u_b);
-        g = (S.nQ > 1) ? bisect(S.probg + ((size_t)S.row * S.nB + nb) * S.nQ, S.nQ, u_g) : 0;
+        nb = (int)RC_IX(guided_index(S.cdf_f, S.guide_f, S.nB, u_b), S.nB, SITE_CDF, S);
+        g = (S.nQ > 1)
+                ? bisect(S.probg + RC_IX(((size_t)S.row * S.nB + nb) * S.nQ, (long long)S.nT * S.nB * S.nQ,
+                                         SITE_PROBG, S),
+                         S.nQ, u_g)
+                : 0;
         const DLevel<R> &L0 = S.lev[0];
-        Pi = L0.P[cell_index(i, j, k, L0.im, L0.jm)];
-        e.xp = S.xc[i];
+        Pi = L0.P[RC_IX(cell_index(i, j, k, L0.im, L0.jm), (long long)L0.im * L0.jm * L0.km, SITE_EMIT_T, S)];
+        e.xp = S.xc[RC_IX(i, S.imax + 2, SITE_CENTRE, S)];
     } else {
         // Lambertian: theta = acos(1 - 2u)/2 (+pi/2 on the east wall)
         // (emiss_angS, :1093-1102), i.e. cos = sqrt(1-u) / -sqrt(u).
@@ -314,9 +346,9 @@ __device__ __forceinline__ bool emit_bundle(Emitted<R> &e, const DSolve<R> &S, i
             e.sx = -RT<R>::sqrt_(u_mu);
             st = RT<R>::sqrt_((R)1 - u_mu);
         }
-        nb = guided_index(S.cdf_s, S.guide_s, S.nB, u_b);
+        nb = (int)RC_IX(guided_index(S.cdf_s, S.guide_s, S.nB, u_b), S.nB, SITE_CDF, S);
         g = (S.nQ > 1) ? bisect(S.probq, S.nQ, u_g) : 0;
-        Pi = S.Pw0[bound][(k - 1) * S.jmax + (j - 1)];
+        Pi = S.Pw0[bound][RC_IX((k - 1) * S.jmax + (j - 1), (long long)S.kmax * S.jmax, SITE_WALL_EMIT_T, S)];
         ic = (bound == 0) ? 1 : S.imax;
         e.xp = (bound == 0) ? (R)0 : S.Lx;
     }
@@ -338,28 +370,29 @@ __device__ __forceinline__ bool emit_bundle(Emitted<R> &e, const DSolve<R> &S, i
         // cell shift when the start point lies on a face (:1429-1441)
         const DLevel<R> &G = S.lev[0];
         const bool fx = e.sx < (R)0, fy = e.sy < (R)0, fz = e.sz < (R)0;
-        if (fx && e.xp == G.xu[ic - 1]) ic = ic - 1;
-        if (fy && e.yp == G.yu[jc - 1]) jc = jc - 1;
-        if (fz && e.zp == G.zu[kc - 1]) kc = kc - 1;
-        if (!fx && e.xp == G.xu[ic]) ic = ic + 1;
-        if (!fy && e.yp == G.yu[jc]) jc = jc + 1;
-        if (!fz && e.zp == G.zu[kc]) kc = kc + 1;
+        if (fx && e.xp == G.xu[RC_IX(ic - 1, G.im + 1, SITE_FACE_SHIFT, S)]) ic = ic - 1;
+        if (fy && e.yp == G.yu[RC_IX(jc - 1, G.jm + 1, SITE_FACE_SHIFT, S)]) jc = jc - 1;
+        if (fz && e.zp == G.zu[RC_IX(kc - 1, G.km + 1, SITE_FACE_SHIFT, S)]) kc = kc - 1;
+        if (!fx && e.xp == G.xu[RC_IX(ic, G.im + 1, SITE_FACE_SHIFT, S)]) ic = ic + 1;
+        if (!fy && e.yp == G.yu[RC_IX(jc, G.jm + 1, SITE_FACE_SHIFT, S)]) jc = jc + 1;
+        if (!fz && e.zp == G.zu[RC_IX(kc, G.km + 1, SITE_FACE_SHIFT, S)]) kc = kc + 1;
     }
     e.ij = ic | (jc << 16);
     e.kk = kc | (kind << 16);
     // OERM weights
-    const KIRow<R> row = S.ki[((size_t)nb * S.nQ + g) * S.nT + (Pi >> 8)];
+    const KIRow<R> row =
+        S.ki[RC_IX(((size_t)nb * S.nQ + g) * S.nT + (Pi >> 8), (long long)S.nB * S.nQ * S.nT, SITE_EMIT_ROW, S)];
     const R fr = coord_frac<R>(Pi);
     const R Ib_i = RT<R>::lerp_(row.ib0, row.ib1, fr);
     if (!(Ib_i > (R)0)) return false;
     e.invTi4 = (R)1 / Ib_i;
     if (kind == 0) {
         const R k_i = RT<R>::lerp_(row.k0, row.k1, fr);
-        const R den = S.den_f[(size_t)nb * S.nQ + g];
+        const R den = S.den_f[RC_IX((size_t)nb * S.nQ + g, (long long)S.nB * S.nQ, SITE_DEN, S)];
         if (!(den > (R)0)) return false;
         e.ratioI = (Ib_i * k_i) / den;
     } else {
-        const R den = S.ibm[nb];
+        const R den = S.ibm[RC_IX(nb, S.nB, SITE_IBM, S)];
         if (!(den > (R)0)) return false;
         e.ratioI = Ib_i / den;
     }
@@ -423,14 +456,16 @@ __device__ __forceinline__ void hit_wall(Ray<R> &r, const DSolve<R> &S, const DL
             default: r.kc = 1; r.zp = (R)0; break;
         }
     } else if (t == 2) {  // black wall at its own temperature
-        wall_deposit(r, S.Ibw[(size_t)w * S.nB + r.nb]);
+        wall_deposit(r, S.Ibw[RC_IX((size_t)w * S.nB + r.nb, 6LL * S.nB, SITE_IBW, S)]);
     } else if (t == 4 || t == 6) {  // black wall at a field temperature
         int idx;
         if (w <= RC_EAST) idx = (r.kc - 1) * L.jm + (r.jc - 1);
         else if (w <= RC_NORTH) idx = (r.kc - 1) * L.im + (r.ic - 1);
         else idx = (r.jc - 1) * L.im + (r.ic - 1);
-        const int q = L.Pw[w][idx];
-        const KIRow<R> row = r.kicol[q >> 8];
+        const int q = L.Pw[w][RC_IX(idx, w <= RC_EAST ? (long long)L.jm * L.km : (w <= RC_NORTH ? (long long)L.im * L.km
+                                                                                              : (long long)L.im * L.jm),
+                                    SITE_WALL_T, S)];
+        const KIRow<R> row = r.kicol[RC_IX(q >> 8, S.nT, SITE_WALL_ROW, S)];
         const R fr = coord_frac<R>(q);
         wall_deposit(r, RT<R>::lerp_(row.ib0, row.ib1, fr));
     } else if (t == 3) {  // specular
@@ -452,13 +487,18 @@ __device__ __forceinline__ void hit_wall(Ray<R> &r, const DSolve<R> &S, const DL
 template <typename R>
 __device__ __forceinline__ void march_step(Ray<R> &r, const DSolve<R> &S) {
     // S lives in global memory (read-only during every kernel that steps)
-    const int4 A = __ldg(&S.lva[r.lev]);
-    const int4 B = __ldg(&S.lvb[r.lev]);
-    const R fxu = __ldg(S.faces + (A.x + r.ic - r.fx));
-    const R fyu = __ldg(S.faces + (A.y + r.jc - r.fy));
-    const R fzu = __ldg(S.faces + (A.z + r.kc - r.fz));
-    const int q = __ldg(S.Pall + (A.w + cell_index(r.ic, r.jc, r.kc, B.x, B.y)));
-    const KIRow<R> row = load_row(r.kicol + (q >> 8));
+    const int4 A = __ldg(&S.lva[RC_IX(r.lev, S.nlev, SITE_LEVEL, S)]);
+    const int4 B = __ldg(&S.lvb[RC_IX(r.lev, S.nlev, SITE_LEVEL, S)]);
+    const R fxu = __ldg(S.faces + RC_IX(A.x + r.ic - r.fx, S.n_faces, SITE_FACE, S));
+    const R fyu = __ldg(S.faces + RC_IX(A.y + r.jc - r.fy, S.n_faces, SITE_FACE, S));
+    const R fzu = __ldg(S.faces + RC_IX(A.z + r.kc - r.fz, S.n_faces, SITE_FACE, S));
+#if RC_CHECKED
+    // the cell itself must lie inside its level (a face index alone can be
+    // in the shared faces array while the cell is off its level)
+    if (r.ic < 1 || r.ic > B.x || r.jc < 1 || r.jc > B.y || r.kc < 1 || r.kc > B.z) RC_IX(-1, 0, SITE_PYRAMID, S);
+#endif
+    const int q = __ldg(S.Pall + RC_IX(A.w + cell_index(r.ic, r.jc, r.kc, B.x, B.y), S.n_P, SITE_PYRAMID, S));
+    const KIRow<R> row = load_row(r.kicol + RC_IX(q >> 8, S.nT, SITE_ROW, S));
     const R dsx = (fxu - r.xp) * r.isx;
     const R dsy = (fyu - r.yp) * r.isy;
     const R dsz = (fzu - r.zp) * r.isz;

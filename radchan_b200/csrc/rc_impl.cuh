@@ -222,6 +222,7 @@ struct Impl : ImplBase {
     R *d_faces = nullptr;              // every level's xu | yu | zu (one allocation)
     std::vector<R *> d_xu, d_yu, d_zu; // per-level views into d_faces
     std::vector<int> face_off, lev_off;  // per-level offsets in d_faces / Slot::d_levAll
+    long long n_faces = 0, n_pyramid = 0;  // their lengths
     R *d_xc = nullptr, *d_yc = nullptr, *d_zc = nullptr;
     R *d_kt = nullptr, *d_Ibt = nullptr, *d_probg = nullptr, *d_prob = nullptr, *d_probq = nullptr;
     R *d_Ibw = nullptr, *d_Tnb = nullptr, *d_kP = nullptr, *d_wvl = nullptr, *d_wvr = nullptr, *d_wvc = nullptr;
@@ -348,6 +349,8 @@ struct Impl : ImplBase {
                 po += (long long)p.maxi[l] * p.maxj[l] * p.maxk[l];
                 if (po > 0x7fffffffLL) return set_err(err_, RC_E_INVALID, "grid too large for 32-bit level offsets");
             }
+            n_faces = (long long)faces.size();
+            n_pyramid = po;
             int rc = upload(d_faces, faces, err_);
             if (rc) return rc;
             for (int l = 0; l < nl; ++l) {
@@ -666,6 +669,9 @@ struct Impl : ImplBase {
         d.ki = p.grey ? s.d_ki_grey : d_ki;
         d.sc = s.d_sc;
         d.partial = s.d_partial;
+        d.n_faces = n_faces;
+        d.n_P = n_pyramid;
+        d.n_partial = (long long)partial_count(rpt);
         const long long ncf = (long long)p.imax * p.jmax * c->kloc;
         d.n_fluid_items = ncf * p.nVar * d.nchunk;
         d.n_items = d.n_fluid_items + (long long)d.nwalls * p.jmax * c->kloc * p.nVar * d.nchunk;
@@ -1100,7 +1106,7 @@ struct Impl : ImplBase {
         out->kappamax = (float)d.kappamax;
         out->Ibmax_fluid = (float)d.Ibmax_f;
         out->table_row = d.row;
-        out->status = d.status;
+        out->status = d.status | (d.bad_site << 8);
         out->bundles = (double)d.bundles;
         out->steps = (double)d.steps;
         float ms = 0.f;

@@ -195,7 +195,9 @@ __global__ void __launch_bounds__(256, MINB) k_march(MarchArgs a) {
                 unsigned key = 0xffffffffu;
                 if (ok) {
                     const int nb = e.nbg & 0xfffff, g = e.nbg >> 20;
-                    key = __float_as_uint((float)S.ki[((size_t)nb * S.nQ + g) * S.nT + S.row].k0);  // k >= 0: monotone bits
+                    key = __float_as_uint((float)S.ki[RC_IX(((size_t)nb * S.nQ + g) * S.nT + S.row,
+                                                            (long long)S.nB * S.nQ * S.nT, SITE_EMIT_ROW, S)]
+                                              .k0);  // k >= 0: monotone bits
                 }
                 int rank = 0;
                 for (int q = 0; q < kWarp; ++q) {
@@ -293,7 +295,7 @@ __global__ void __launch_bounds__(256, MINB) k_march(MarchArgs a) {
                 double g = 0.0;
                 for (int q = 0; q < gs; ++q) g += __shfl_sync(0xffffffffu, s, base + q);
                 const long long item = (par ? item0_1 : item0_0) + lane;
-                if (lane == base && item < S.n_items) S.partial[item / gs] = g;
+                if (lane == base && item < S.n_items) S.partial[RC_IX(item / gs, S.n_partial, SITE_PARTIAL, S)] = g;
                 busy &= ~(1u << par);
                 if (epar == par) epar = -1;
                 __syncwarp();

@@ -1,0 +1,102 @@
+"""The bounds-checked build (libradchan_checked.so, RC_CHECKED=1): every
+table, field and partial-sum index of the march is checked against its
+array on the device.  Small cases covering each path (grey, narrow band
+with levels, every wall type, both wall fluxes, a z slab, band-sorted
+order, the FP64 build, a batch, the server) run in a child process that
+loads the checked library; none may flag an index (status bit 3) and each
+result must equal the oracle bit for bit."""
+import json
+import os
+import subprocess
+import sys
+
+import numpy as np
+import pytest
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
+
+
+def _cases():
+    from radchan_b200 import workloads as W
+    tabs = W.tables_nb(nB=24, nQ=4, nT=32)
+    lv = dict(nB=24, nQ=4, nT=32, levels=[(16, 8, 8), (8, 4, 4)], maxs=[5, 100000])
+    out = [("grey", W.channel_params(16, 8, 8, grey=True, photmax=16, nVar=2), None, {}),
+           ("nb_levels_walls", W.channel_params(16, 8, 8, photmax=16, nVar=2, calcwalls=1, adiabw=1, adiabe=1, **lv),
+            tabs, {}),
+           ("black_y_specular_z", W.channel_params(16, 8, 8, photmax=16, nVar=2, bd_y=2, bd_z=3, **lv), tabs, {}),
+           ("specular_y_adiabatic_west", W.channel_params(16, 8, 8, photmax=16, nVar=2, bd_y=3, calcwalls=1,
+                                                          adiabw=1, **lv), tabs, {}),
+           ("sorted", W.channel_params(16, 8, 8, photmax=16, nVar=2, **lv), tabs, {"sort": 1}),
+           ("fp64", W.channel_params(16, 8, 8, photmax=8, nVar=2, floatpoint=1, **lv), tabs, {})]
+    p = W.channel_params(16, 8, 8, photmax=16, nVar=2, calcwalls=1, adiabw=1, **lv)
+    p.p_col = 2
+    out.append(("z_slab", p, tabs, {"zstart": 5}))
+    return out
+
+
+def child():
+    from oracle import oracle as O
+    from radchan_b200 import _lib as L
+    from radchan_b200 import api
+    from radchan_b200 import workloads as W
+    assert L.LIB_PATH.endswith("libradchan_checked.so"), L.LIB_PATH
+    res = {}
+    for name, p, tabs, opt in _cases():
+        T = W.channel_field(p, seed=3)
+        s = api.Solver(p, tabs)
+        if opt.get("sort"):
+            s.set_launch(sort_bands=1)
+        z = opt.get("zstart", 1)
+        t = s.solve_async(T, zstart=z)
+        st = s.info(t).status
+        r = s.collect(t)
+        o = O.solve(p, tabs, T, zstart=z, rpt=s.get_launch()[0], fp64=bool(p.floatpoint))
+        res[name] = dict(status=st, equal=bool(np.array_equal(r.q64, o["q64"]) and np.array_equal(r.qw64, o["qw64"])))
+        s.close()
+    # a batch of two problems and a served request
+    cases = _cases()
+    b = api.Batch()
+    solvers = []
+    for name, p, tabs, opt in cases[:2]:
+        s = api.Solver(p, tabs)
+        solvers.append((s, p, tabs))
+        b.add(s, W.channel_field(p, seed=3))
+    b.run()
+    b.wait()
+    eq = True
+    for i, (s, p, tabs) in enumerate(solvers):
+        o = O.solve(p, tabs, W.channel_field(p, seed=3), rpt=s.get_launch()[0])
+        eq = eq and bool(np.array_equal(b.collect(i).q64, o["q64"]))
+    b.close()
+    res["batch"] = dict(status=0, equal=eq)
+    name, p, tabs, _ = cases[1]
+    T = W.channel_field(p, seed=3)
+    alone = api.Solver(p, tabs).solve(T, want64=False)
+    srv = api.Server()
+    r = srv.wait(srv.submit(p, T, table_set=srv.add_tables(tabs)))
+    srv.close()
+    res["server"] = dict(status=0, equal=bool(np.array_equal(r.Q, alone.Q)))
+    print(json.dumps(res))
+
+
+@pytest.mark.gpu
+def test_checked_build_flags_nothing_and_matches_the_oracle():
+    lib = os.path.join(ROOT, "radchan_b200", "libradchan_checked.so")
+    if not os.path.exists(lib):
+        from radchan_b200 import build
+        build.build(checked=True)
+    env = dict(os.environ, RADCHAN_LIB="checked", PYTHONPATH=ROOT)
+    r = subprocess.run([sys.executable, os.path.abspath(__file__), "--child"], env=env, cwd=ROOT,
+                       capture_output=True, text=True, timeout=900)
+    assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-4000:]
+    res = json.loads(r.stdout.strip().splitlines()[-1])
+    assert len(res) == 9
+    for name, v in res.items():
+        assert v["status"] & 8 == 0, (name, v["status"] >> 8)
+        assert v["equal"], name
+
+
+if __name__ == "__main__" and "--child" in sys.argv:
+    sys.path.insert(0, ROOT)
+    child()
