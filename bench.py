@@ -560,11 +560,13 @@ def run_ours(args, ws, rank, local):
     if args.rays_per_thread or args.block or args.occupancy or args.sort >= 0:
         s.set_launch(rays_per_thread=args.rays_per_thread, block_threads=args.block, sort_bands=args.sort,
                      occupancy=args.occupancy)
+    if args.prio is not None:
+        s.set_priority(args.prio)
     T_dev = torch.from_numpy(T).to(f"cuda:{dev}")
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=f"cuda:{dev}")
     # k_init_scalars, k_tmax, k_setup1, k_setup2, k_levels, k_patch_desc,
-    # k_march, k_tally (+ k_grey_ib, k_build_ki for a grey gas)
-    kernels_per_solve = 8 + (2 if p.grey else 0)
+    # [k_prio_tiles,] k_march, k_tally (+ k_grey_ib, k_build_ki for a grey gas)
+    kernels_per_solve = 8 + (2 if p.grey else 0) + (0 if args.prio == 0 else 1)
     # warm-up
     for _ in range(args.warmup):
         t = s.solve_device_async(T_dev.data_ptr())
@@ -665,6 +667,8 @@ def main():
     ap.add_argument("--block", type=int, default=0)
     ap.add_argument("--occupancy", type=int, default=0)
     ap.add_argument("--sort", type=int, default=-1, help="band-sorted bundle order 0/1 (default: context's)")
+    ap.add_argument("--prio", type=float, default=None,
+                    help="long-ray priority threshold on |s_x| (0: off; default: context's)")
     ap.add_argument("--ref-seconds", dest="ref_seconds", type=float, default=12.0)
     ap.add_argument("--traffic", type=float, default=None)
     ap.add_argument("--photmax", type=int, default=0, help="override bundles per cell (profiling runs)")

@@ -123,6 +123,7 @@ _SIGS = [
     ("rc_device_results", _I, [_VP, C.c_int32, C.POINTER(_VP), C.POINTER(_VP), C.POINTER(_VP), C.POINTER(_VP)]),
     ("rc_solve_info_get", _I, [_VP, C.c_int32, C.POINTER(RcSolveInfo)]),
     ("rc_set_launch", _I, [_VP, _I, _I, _I, _I]),
+    ("rc_set_priority", _I, [_VP, C.c_float]),
     ("rc_get_launch", _I, [_VP, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int)]),
     ("rc_autotune", _I, [_VP, _FP, _I, _I, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int),
                          C.POINTER(C.c_int)]),

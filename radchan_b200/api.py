@@ -230,6 +230,11 @@ class Solver:
     def set_launch(self, rays_per_thread=0, block_threads=0, sort_bands=-1, occupancy=0):
         L.check(L.lib().rc_set_launch(self.ctx, rays_per_thread, block_threads, sort_bands, occupancy), self.ctx)
 
+    def set_priority(self, threshold: float):
+        """rc_set_priority: tiles holding a bundle with |s_x| < threshold
+        are marched first (0 turns it off); results do not change."""
+        L.check(L.lib().rc_set_priority(self.ctx, float(threshold)), self.ctx)
+
     def get_launch(self):
         """(rays_per_thread, block_threads, sort_bands, occupancy)"""
         a, b, c, d = C.c_int(), C.c_int(), C.c_int(), C.c_int()

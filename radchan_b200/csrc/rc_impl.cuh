@@ -168,6 +168,10 @@ struct SlotCommon {
     long long *d_tiles = nullptr, *h_tiles = nullptr;
     unsigned long long *d_counter = nullptr;
     TallyOut *d_out = nullptr, *h_out = nullptr;
+    // long-ray priority list (k_prio_tiles): listed tiles, per-tile flag, count
+    unsigned *d_prio = nullptr, *d_nprio = nullptr;
+    unsigned char *d_tprio = nullptr;
+    long long prio_cap = 0;
     int state = 0;  // 0 free, 1 in flight, 2 finished (results pending)
     rc_ticket ticket = -1;
     int zstart = 1;
@@ -187,6 +191,7 @@ struct rc_ctx {
     int next_ticket = 1;
     // launch knobs
     int rpt = 8, block = 256, sort = 0, minb = 3;
+    float prio_thr = 1e-3f;  // long-ray priority: |s_x| below this marks a tile (0: off)
     int num_sms = 148;
     bool has_tables = false;
     // DNS-coupling scratch (rc_dns_source): T1 pencil + four outputs, and a counter
@@ -284,6 +289,10 @@ struct Impl : ImplBase {
             dfree(s.d_counter);
             dfree(s.d_out);
             hfree(s.h_out);
+            dfree(s.d_prio);
+            dfree(s.d_tprio);
+            dfree(s.d_nprio);
+            s.prio_cap = 0;
             dfree(s.d_levAll);
             s.d_levT.clear();
             for (int l = 0; l < RC_MAX_LEVELS; ++l)
@@ -768,8 +777,36 @@ struct Impl : ImplBase {
         return minb <= 2 ? k_march<R, 2> : minb == 3 ? k_march<R, 3> : k_march<R, 4>;
     }
 
+    // Long-ray priority list of a one-solve launch (k_prio_tiles) on stream
+    // st, into the slot's buffers; `use` stays false when the knob is off or
+    // the solve has more tiles than the list is kept for (its tail is then
+    // a small share of the launch).
+    static constexpr long long kPrioMaxTiles = 1LL << 25;
+    int enqueue_prio(Slot<R> &s, cudaStream_t st, bool &use) {
+        std::string *err_ = &c->err;
+        use = false;
+        const long long nt = s.h_desc->n_tiles;
+        if (!(c->prio_thr > 0.f) || nt < 1 || nt > kPrioMaxTiles) return RC_OK;
+        if (s.prio_cap < nt) {
+            dfree(s.d_prio);
+            dfree(s.d_tprio);
+            s.prio_cap = 0;
+            RC_CK(cudaMalloc((void **)&s.d_prio, nt * sizeof(unsigned)));
+            RC_CK(cudaMalloc((void **)&s.d_tprio, nt));
+            s.prio_cap = nt;
+        }
+        if (!s.d_nprio) RC_CK(cudaMalloc((void **)&s.d_nprio, sizeof(unsigned)));
+        RC_CK(cudaMemsetAsync(s.d_nprio, 0, sizeof(unsigned), st));
+        const long long grid = std::max<long long>(1, std::min<long long>((nt + 7) / 8, (long long)c->num_sms * 16));
+        k_prio_tiles<R><<<(unsigned)grid, 256, 0, st>>>(s.d_desc, (R)c->prio_thr, s.d_prio, s.d_tprio, s.d_nprio);
+        RC_CK(cudaGetLastError());
+        use = true;
+        return RC_OK;
+    }
+
     int launch_march(const DSolve<R> *d_solves, const long long *d_tiles, int nsolves, long long total_tiles,
-                     unsigned long long *d_counter, int block, int rpt_max, cudaStream_t st, int minb = 0) {
+                     unsigned long long *d_counter, int block, int rpt_max, cudaStream_t st, int minb = 0,
+                     const Slot<R> *prio = nullptr) {
         std::string *err_ = &c->err;
         RC_FAILPOINT("march");
         if (minb <= 0) minb = c->minb;
@@ -790,6 +827,9 @@ struct Impl : ImplBase {
         a.total_tiles = total_tiles;
         a.tile_counter = d_counter;
         a.rpt_max = rpt_max;
+        a.prio_tiles = prio ? prio->d_prio : nullptr;
+        a.tile_prio = prio ? prio->d_tprio : nullptr;
+        a.n_prio = prio ? prio->d_nprio : nullptr;
         fn<<<(unsigned)grid, block, smem, st>>>(a);
         RC_CK(cudaGetLastError());
         return RC_OK;
@@ -896,7 +936,11 @@ struct Impl : ImplBase {
         s.h_tiles[1] = s.h_desc->n_tiles;
         RC_CK(cudaMemcpyAsync(s.d_tiles, s.h_tiles, 2 * sizeof(long long), cudaMemcpyHostToDevice, s.st));
         RC_CK(cudaEventRecord(s.e_march0, s.st));
-        rc = launch_march(s.d_desc, s.d_tiles, 1, s.h_desc->n_tiles, s.d_counter, c->block, rpt, s.st);
+        bool prio = false;
+        rc = enqueue_prio(s, s.st, prio);
+        if (rc) return rc;
+        rc = launch_march(s.d_desc, s.d_tiles, 1, s.h_desc->n_tiles, s.d_counter, c->block, rpt, s.st, 0,
+                          prio ? &s : nullptr);
         if (rc) return rc;
         RC_CK(cudaEventRecord(s.e_march1, s.st));
         rc = launch_tally(s.d_desc, s.d_out, 1, tally_cells(), s.st);
@@ -925,7 +969,11 @@ struct Impl : ImplBase {
             s.h_tiles[1] = s.h_desc->n_tiles;
             RC_CK(cudaMemcpyAsync(s.d_tiles, s.h_tiles, 2 * sizeof(long long), cudaMemcpyHostToDevice, s.st));
             RC_CK(cudaEventRecord(s.e_march0, s.st));
-            rc = launch_march(s.d_desc, s.d_tiles, 1, s.h_desc->n_tiles, s.d_counter, block, rpt, s.st, minb);
+            bool prio = false;
+            rc = enqueue_prio(s, s.st, prio);
+            if (rc) return rc;
+            rc = launch_march(s.d_desc, s.d_tiles, 1, s.h_desc->n_tiles, s.d_counter, block, rpt, s.st, minb,
+                              prio ? &s : nullptr);
             if (rc) return rc;
             RC_CK(cudaEventRecord(s.e_march1, s.st));
             RC_CK(cudaEventSynchronize(s.e_march1));

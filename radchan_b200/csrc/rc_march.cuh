@@ -39,7 +39,53 @@ struct MarchArgs {
     long long total_tiles;
     unsigned long long *tile_counter;
     int rpt_max;
+    // long-ray priority (one solve only; NULL: tiles in natural order): the
+    // first *n_prio claims take prio_tiles[], the rest take the natural
+    // order and skip the tiles whose tile_prio byte is set
+    const unsigned *prio_tiles;
+    const unsigned char *tile_prio;
+    const unsigned *n_prio;
 };
+
+// Tiles holding a bundle emitted within `thr` of the x-wall planes
+// (|s_x| < thr): in a near-transparent band such a ray runs between the
+// periodic y/z boundaries for up to the last level's step budget, so a
+// launch that meets it late idles while it finishes.  One warp per tile
+// draws the same direction uniform as the emission (Philox counter of the
+// bundle, emit_bundle) for each of the tile's bundles; tiles with a
+// candidate are listed (in any order) and flagged.  Only the order in which
+// tiles are claimed changes, never a result.
+template <typename R>
+__global__ void k_prio_tiles(const DSolve<R> *Sp, R thr, unsigned *prio_tiles, unsigned char *tile_prio,
+                             unsigned *n_prio) {
+    const DSolve<R> &S = *Sp;
+    const int lane = threadIdx.x & 31;
+    const long long nw = (long long)gridDim.x * (blockDim.x >> 5);
+    const R thr2 = thr * thr;
+    for (long long tile = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); tile < S.n_tiles;
+         tile += nw) {
+        const ItemId it = decode_item(S, tile * kWarp + lane);
+        bool cand = false;
+        if (it.kind >= 0) {
+            const uint32_t cell = (it.kind == 0)
+                                      ? (uint32_t)((it.i - 1) + S.imax * ((it.j - 1) + S.jmax * (it.k - 1)))
+                                      : (uint32_t)((it.j - 1) + S.jmax * (it.k - 1));
+            const int h1 = min(it.h0 + S.rpt, S.photmax);
+            for (int h = it.h0; h < h1; ++h) {
+                const rc_u32x4 d = bundle_draws(S.key0, S.key1, h, it.v, it.kind, cell);
+                const R u = (R)rc_u01(d.y);
+                if (it.kind == 0) cand = cand || RT<R>::fabs_((R)1 - (R)2 * u) < thr;  // s_x = 1 - 2u
+                else if (it.kind == 1) cand = cand || (R)1 - u < thr2;                 // s_x = sqrt(1 - u)
+                else cand = cand || u < thr2;                                           // s_x = -sqrt(u)
+            }
+        }
+        const unsigned m = __ballot_sync(0xffffffffu, cand);
+        if (lane == 0) {
+            tile_prio[tile] = m != 0u;
+            if (m) prio_tiles[atomicAdd(n_prio, 1u)] = (unsigned)tile;
+        }
+    }
+}
 
 template <typename R>
 struct WarpShared {
@@ -97,7 +143,10 @@ __global__ void __launch_bounds__(256, MINB) k_march(MarchArgs a) {
     unsigned long long pending = ~0ull;  // fetched tile waiting for a solve switch
     // tiles claimed from the queue but not started: [chunk_next, chunk_end)
     unsigned long long chunk_next = 0, chunk_end = 0;
-    const unsigned long long total = (unsigned long long)a.total_tiles;
+    // with the long-ray priority list, the claim space is the listed tiles
+    // followed by all tiles in natural order (listed ones skipped there)
+    const unsigned long long nprio = a.n_prio ? (unsigned long long)__ldg(a.n_prio) : 0ull;
+    const unsigned long long total = (unsigned long long)a.total_tiles + nprio;
     const unsigned long long all_warps = (unsigned long long)gridDim.x * nwarps;
     // lanes tracing a ray, and lanes whose ray belongs to buffer 1
     // (warp-uniform; kept in step with the lanes' own flags)
@@ -134,8 +183,15 @@ __global__ void __launch_bounds__(256, MINB) k_march(MarchArgs a) {
                         chunk_next = c0;
                     }
                     tile = chunk_next < chunk_end ? chunk_next++ : total;
+                    if (a.n_prio && tile < total) {
+                        if (tile < nprio) tile = __ldg(a.prio_tiles + tile);
+                        else if (__ldg(a.tile_prio + (tile - nprio))) tile = ~1ull;  // taken from the list
+                        else tile -= nprio;
+                    }
                 }
-                if (tile >= (unsigned long long)a.total_tiles) {
+                if (tile == ~1ull) {
+                    // a listed tile met again in natural order: nothing this round
+                } else if (tile >= (unsigned long long)a.total_tiles) {
                     drained = true;
                     pending = ~0ull;
                 } else {

@@ -223,6 +223,13 @@ int rc_set_launch(rc_ctx *c, int rays_per_thread, int block_threads, int sort_ba
     return RC_OK;
 }
 
+int rc_set_priority(rc_ctx *c, float threshold) {
+    if (!c) return set_err(nullptr, RC_E_INVALID, "NULL context");
+    if (!(threshold >= 0.f) || threshold > 1.f) return set_err(&c->err, RC_E_INVALID, "threshold must be in [0, 1]");
+    c->prio_thr = threshold;
+    return RC_OK;
+}
+
 int rc_get_launch(rc_ctx *c, int *rays_per_thread, int *block_threads, int *sort_bands, int *occupancy) {
     if (!c) return set_err(nullptr, RC_E_INVALID, "NULL context");
     if (rays_per_thread) *rays_per_thread = c->rpt;

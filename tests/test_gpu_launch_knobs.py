@@ -37,6 +37,36 @@ def test_sort_block_occupancy_leave_result_unchanged(grey):
     s.close()
 
 
+@pytest.mark.parametrize("grey", [True, False])
+def test_long_ray_priority_changes_order_not_results(grey):
+    """Tiles with near-grazing bundles marched first (rc_set_priority): the
+    same bundles, steps and bit-identical results for any threshold, off
+    included, and equal to the oracle."""
+    from oracle import oracle as O
+    if grey:
+        p, tabs, T = W.config_grey_32(photmax=32), None, W.channel_field(W.config_grey_32(), seed=5)
+    else:
+        p, tabs, T = _nb_case()
+    s = api.Solver(p, tabs)
+    runs = []
+    for thr in (0.0, 1e-3, 0.05, 1.0):
+        s.set_priority(thr)
+        t = s.solve_async(T)
+        i = s.info(t)
+        runs.append((s.collect(t), i.bundles, i.steps))
+    base, nb, ns = runs[0]
+    for r, b, st in runs[1:]:
+        assert (b, st) == (nb, ns)
+        np.testing.assert_array_equal(r.q64, base.q64)
+        np.testing.assert_array_equal(r.var64, base.var64)
+        np.testing.assert_array_equal(r.qw64, base.qw64)
+    o = O.solve(p, tabs, T, rpt=s.get_launch()[0])
+    np.testing.assert_array_equal(base.q64, o["q64"])
+    with pytest.raises(Exception):
+        s.set_priority(-1.0)
+    s.close()
+
+
 def test_autotune_picks_valid_knobs_and_matches_oracle():
     from oracle import oracle as O
     p, tabs, T = _nb_case()
