@@ -216,13 +216,15 @@ int rc_solve_info_get(rc_ctx *ctx, rc_ticket ticket, rc_solve_info *info);
 int rc_set_launch(rc_ctx *ctx, int rays_per_thread, int block_threads, int sort_bands, int occupancy);
 int rc_get_launch(rc_ctx *ctx, int *rays_per_thread, int *block_threads, int *sort_bands, int *occupancy);
 /* Long-ray priority of rc_solve_async / rc_solve_device_async (default
- * 1e-3; 0 turns it off).  A bundle emitted with |s_x| below the threshold,
+ * 4e-3; 0 turns it off).  A bundle emitted with |s_x| below the threshold,
  * nearly parallel to the x walls, can cross the periodic y/z boundaries
  * for up to the last level's step budget in a near-transparent band.  Such
  * a ray started late in a launch keeps the GPU waiting for it alone.
  * Before the march, a short pass draws every bundle's direction and the
  * tiles holding such a bundle are marched first.  It changes the order of
- * the work, never a result.  Solves of more than 2^25 tiles skip it. */
+ * the work, never a result.  It runs only when no other solve of the
+ * context is still running on the device (that solve fills the tail
+ * anyway), and solves of more than 2^25 tiles skip it. */
 int rc_set_priority(rc_ctx *ctx, float threshold);
 /* Try launch configurations on T (host) with a reduced bundle count
  * (pilot_photmax; <= 0: the context's photmax) and keep the fastest:

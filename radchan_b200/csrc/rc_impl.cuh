@@ -191,7 +191,7 @@ struct rc_ctx {
     int next_ticket = 1;
     // launch knobs
     int rpt = 8, block = 256, sort = 0, minb = 3;
-    float prio_thr = 1e-3f;  // long-ray priority: |s_x| below this marks a tile (0: off)
+    float prio_thr = 4e-3f;  // long-ray priority: |s_x| below this marks a tile (0: off)
     int num_sms = 148;
     bool has_tables = false;
     // DNS-coupling scratch (rc_dns_source): T1 pencil + four outputs, and a counter
@@ -935,10 +935,17 @@ struct Impl : ImplBase {
         s.h_tiles[0] = 0;
         s.h_tiles[1] = s.h_desc->n_tiles;
         RC_CK(cudaMemcpyAsync(s.d_tiles, s.h_tiles, 2 * sizeof(long long), cudaMemcpyHostToDevice, s.st));
+        // the long-ray priority pays only when this solve is alone on the
+        // device: a solve still running in the other slot overlaps its tail
+        bool alone = true;
+        for (auto &o : slots)
+            if (&o != &s && o.state == 1 && cudaEventQuery(o.e1) == cudaErrorNotReady) alone = false;
         RC_CK(cudaEventRecord(s.e_march0, s.st));
         bool prio = false;
-        rc = enqueue_prio(s, s.st, prio);
-        if (rc) return rc;
+        if (alone) {
+            rc = enqueue_prio(s, s.st, prio);
+            if (rc) return rc;
+        }
         rc = launch_march(s.d_desc, s.d_tiles, 1, s.h_desc->n_tiles, s.d_counter, c->block, rpt, s.st, 0,
                           prio ? &s : nullptr);
         if (rc) return rc;
