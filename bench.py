@@ -565,8 +565,10 @@ def run_ours(args, ws, rank, local):
     T_dev = torch.from_numpy(T).to(f"cuda:{dev}")
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=f"cuda:{dev}")
     # k_init_scalars, k_tmax, k_setup1, k_setup2, k_levels, k_patch_desc,
-    # [k_prio_tiles,] k_march, k_tally (+ k_grey_ib, k_build_ki for a grey gas)
-    kernels_per_solve = 8 + (2 if p.grey else 0) + (0 if args.prio == 0 else 1)
+    # k_march, k_tally (+ k_grey_ib, k_build_ki for a grey gas); the
+    # long-ray priority list (k_prio_tiles) is built by the first warm-up
+    # solve and reused, as it does not depend on the field
+    kernels_per_solve = 8 + (2 if p.grey else 0)
     # warm-up
     for _ in range(args.warmup):
         t = s.solve_device_async(T_dev.data_ptr())

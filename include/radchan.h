@@ -222,9 +222,12 @@ int rc_get_launch(rc_ctx *ctx, int *rays_per_thread, int *block_threads, int *so
  * a ray started late in a launch keeps the GPU waiting for it alone.
  * Before the march, a short pass draws every bundle's direction and the
  * tiles holding such a bundle are marched first.  It changes the order of
- * the work, never a result.  It runs only when no other solve of the
- * context is still running on the device (that solve fills the tail
- * anyway), and solves of more than 2^25 tiles skip it. */
+ * the work, never a result.  The list depends on the seed, photmax,
+ * rays_per_thread, replicates and decomposition but not on T, so each solve
+ * slot builds it once and reuses it while those stay the same.  It is used
+ * only when no other solve of the context is still running on the device
+ * (that solve fills the tail anyway), and solves of more than 2^25 tiles
+ * skip it. */
 int rc_set_priority(rc_ctx *ctx, float threshold);
 /* Try launch configurations on T (host) with a reduced bundle count
  * (pilot_photmax; <= 0: the context's photmax) and keep the fastest:

@@ -172,6 +172,9 @@ struct SlotCommon {
     unsigned *d_prio = nullptr, *d_nprio = nullptr;
     unsigned char *d_tprio = nullptr;
     long long prio_cap = 0;
+    // what the list was built for (it does not depend on the field)
+    long long prio_key[10] = {};
+    bool prio_ok = false;
     int state = 0;  // 0 free, 1 in flight, 2 finished (results pending)
     rc_ticket ticket = -1;
     int zstart = 1;
@@ -293,6 +296,7 @@ struct Impl : ImplBase {
             dfree(s.d_tprio);
             dfree(s.d_nprio);
             s.prio_cap = 0;
+            s.prio_ok = false;
             dfree(s.d_levAll);
             s.d_levT.clear();
             for (int l = 0; l < RC_MAX_LEVELS; ++l)
@@ -780,13 +784,29 @@ struct Impl : ImplBase {
     // Long-ray priority list of a one-solve launch (k_prio_tiles) on stream
     // st, into the slot's buffers; `use` stays false when the knob is off or
     // the solve has more tiles than the list is kept for (its tail is then
-    // a small share of the launch).
+    // a small share of the launch).  The list depends only on the bundles'
+    // directions, i.e. on the seed, photmax, rays_per_thread, replicates and
+    // the work decomposition -- never on the temperature field -- so the
+    // slot keeps it and rebuilds it only when one of those changes.
     static constexpr long long kPrioMaxTiles = 1LL << 25;
     int enqueue_prio(Slot<R> &s, cudaStream_t st, bool &use) {
         std::string *err_ = &c->err;
         use = false;
-        const long long nt = s.h_desc->n_tiles;
+        const DSolve<R> &d = *s.h_desc;
+        const long long nt = d.n_tiles;
         if (!(c->prio_thr > 0.f) || nt < 1 || nt > kPrioMaxTiles) return RC_OK;
+        unsigned thr_bits;
+        memcpy(&thr_bits, &c->prio_thr, 4);
+        const long long key[10] = {(long long)d.key0 | ((long long)d.key1 << 32), d.photmax, d.rpt, d.nVar,
+                                   (long long)d.imax | ((long long)d.jmax << 32),
+                                   (long long)d.kloc | ((long long)d.kfirst << 32), nt,
+                                   (long long)d.nwalls | ((long long)d.wall_id[0] << 8) | ((long long)d.wall_id[1] << 16),
+                                   (long long)thr_bits, (long long)sizeof(R)};
+        if (s.prio_ok && s.prio_cap >= nt && memcmp(key, s.prio_key, sizeof(key)) == 0) {
+            use = true;
+            return RC_OK;
+        }
+        s.prio_ok = false;
         if (s.prio_cap < nt) {
             dfree(s.d_prio);
             dfree(s.d_tprio);
@@ -800,6 +820,8 @@ struct Impl : ImplBase {
         const long long grid = std::max<long long>(1, std::min<long long>((nt + 7) / 8, (long long)c->num_sms * 16));
         k_prio_tiles<R><<<(unsigned)grid, 256, 0, st>>>(s.d_desc, (R)c->prio_thr, s.d_prio, s.d_tprio, s.d_nprio);
         RC_CK(cudaGetLastError());
+        memcpy(s.prio_key, key, sizeof(key));
+        s.prio_ok = true;
         use = true;
         return RC_OK;
     }

@@ -49,11 +49,18 @@ def test_long_ray_priority_changes_order_not_results(grey):
         p, tabs, T = _nb_case()
     s = api.Solver(p, tabs)
     runs = []
-    for thr in (0.0, 1e-3, 0.05, 1.0):
+    # 4e-3 twice: the second solve reuses the slot's list (the list depends
+    # on the bundles' directions only); the field changes between them
+    for thr, T_ in ((0.0, T), (1e-3, T), (4e-3, T), (4e-3, T), (0.05, T), (1.0, T)):
         s.set_priority(thr)
-        t = s.solve_async(T)
+        t = s.solve_async(T_)
         i = s.info(t)
         runs.append((s.collect(t), i.bundles, i.steps))
+    T2 = T * np.float32(1.02)
+    s.set_priority(4e-3)
+    r2 = s.solve(T2)
+    s.set_priority(0.0)
+    np.testing.assert_array_equal(s.solve(T2).q64, r2.q64)
     base, nb, ns = runs[0]
     for r, b, st in runs[1:]:
         assert (b, st) == (nb, ns)
