@@ -226,8 +226,8 @@ int rc_get_launch(rc_ctx *ctx, int *rays_per_thread, int *block_threads, int *so
  * rays_per_thread, replicates and decomposition but not on T, so each solve
  * slot builds it once and reuses it while those stay the same.  It is used
  * only when no other solve of the context is still running on the device
- * (that solve fills the tail anyway), and solves of more than 2^25 tiles
- * skip it. */
+ * (that solve fills the tail anyway), and solves of more than 2^22 tiles
+ * skip it (there, reordering cost more than the tail it removed). */
 int rc_set_priority(rc_ctx *ctx, float threshold);
 /* Try launch configurations on T (host) with a reduced bundle count
  * (pilot_photmax; <= 0: the context's photmax) and keep the fastest:

@@ -164,34 +164,42 @@ __global__ void __launch_bounds__(256, MINB) k_march(MarchArgs a) {
             if (!((busy >> fpar) & 1u)) {
                 unsigned long long tile = pending;
                 if (tile == ~0ull) {
-                    if (chunk_next >= chunk_end) {
-                        // guided self-scheduling: claim up to kChunkMax
-                        // consecutive tiles (usually of one solve), so a warp
-                        // keeps two tiles of the same solve in flight; claim
-                        // fewer as the queue drains to keep the tail short
-                        unsigned long long c0 = 0;
-                        if (lane == 0) {
-                            const unsigned long long seen = *(volatile unsigned long long *)a.tile_counter;
-                            const unsigned long long rem = seen < total ? total - seen : 0ull;
-                            const unsigned long long k =
-                                max(1ull, min((unsigned long long)kChunkMax, rem / (4ull * all_warps)));
-                            c0 = atomicAdd(a.tile_counter, k);
-                            chunk_end = min(c0 + k, total);
+                    // ends: every pass advances chunk_next or the shared
+                    // counter, and a claim at or past `total` ends the queue
+                    for (;;) {
+                        if (chunk_next >= chunk_end) {
+                            // guided self-scheduling: claim up to kChunkMax
+                            // consecutive tiles (usually of one solve), so a
+                            // warp keeps two tiles of the same solve in
+                            // flight; claim fewer as the queue drains to keep
+                            // the tail short
+                            unsigned long long c0 = 0;
+                            if (lane == 0) {
+                                const unsigned long long seen = *(volatile unsigned long long *)a.tile_counter;
+                                const unsigned long long rem = seen < total ? total - seen : 0ull;
+                                const unsigned long long k =
+                                    max(1ull, min((unsigned long long)kChunkMax, rem / (4ull * all_warps)));
+                                c0 = atomicAdd(a.tile_counter, k);
+                                chunk_end = min(c0 + k, total);
+                            }
+                            c0 = __shfl_sync(0xffffffffu, c0, 0);
+                            chunk_end = __shfl_sync(0xffffffffu, chunk_end, 0);
+                            chunk_next = c0;
                         }
-                        c0 = __shfl_sync(0xffffffffu, c0, 0);
-                        chunk_end = __shfl_sync(0xffffffffu, chunk_end, 0);
-                        chunk_next = c0;
-                    }
-                    tile = chunk_next < chunk_end ? chunk_next++ : total;
-                    if (a.n_prio && tile < total) {
-                        if (tile < nprio) tile = __ldg(a.prio_tiles + tile);
-                        else if (__ldg(a.tile_prio + (tile - nprio))) tile = ~1ull;  // taken from the list
-                        else tile -= nprio;
+                        tile = chunk_next < chunk_end ? chunk_next++ : total;
+                        if (!a.n_prio || tile >= total) break;
+                        if (tile < nprio) {
+                            tile = __ldg(a.prio_tiles + tile);
+                            break;
+                        }
+                        if (!__ldg(a.tile_prio + (tile - nprio))) {
+                            tile -= nprio;
+                            break;
+                        }
+                        // a listed tile met again in natural order: claim the next
                     }
                 }
-                if (tile == ~1ull) {
-                    // a listed tile met again in natural order: nothing this round
-                } else if (tile >= (unsigned long long)a.total_tiles) {
+                if (tile >= (unsigned long long)a.total_tiles) {
                     drained = true;
                     pending = ~0ull;
                 } else {
