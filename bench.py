@@ -33,7 +33,10 @@ Legs on one GPU (skipped with --no-legs):
 --precision runs the FP32-march vs FP64-build study at 192x128x128.
 
 --impl reference times the CPU restatement of the reference's ray loop
-(the reference has no CPU implementation of this path) on all host cores.
+(the reference has no CPU implementation of this path) on all host cores,
+on inputs the oracle builds itself (the product library is never loaded),
+and then the reference's own CUDA build on the same GPU (ref_cuda: each
+solve in a child process, since get_results_ resets the device).
 """
 from __future__ import annotations
 
@@ -69,23 +72,52 @@ def peaks():
         return 6650.0, "fallback"
 
 
+def workload_desc(name, p):
+    """The config dict of a workload, from its parameter set (either the
+    product's or the oracle's rc_params mirror)."""
+    if name == "nb64":
+        return dict(workload="narrow-band 100x8 OERM, 64^3 channel, 3 levels 64/32/16 maxs 5/5/1e5, photmax %d, "
+                             "nVar 4, srt 1, calcwalls (adiabatic west wall)" % p.photmax,
+                    grid=[64, 64, 64], bands=100, gpoints=8, temps=64, photmax=p.photmax, nVar=4, levels=3)
+    if name == "grey32":
+        return dict(workload="grey OERM kappa=1, 32^3 channel, photmax %d, nVar 4" % p.photmax, grid=[32, 32, 32],
+                    photmax=p.photmax, nVar=4, levels=1)
+    raise SystemExit("unknown workload " + name)
+
+
+def bench_config(desc, ws):
+    """The same config dict in both arms."""
+    return dict(desc, parallelism="replicas" if ws > 1 else "single", l2="flushed between steps")
+
+
 def workload(name, photmax=0):
+    """Seeded inputs built by the product package (this solver's arm)."""
     from radchan_b200 import workloads as W
     if name == "nb64":
         p = W.config_nb_64(photmax=photmax or 256)
         tabs = W.tables_nb()
-        desc = dict(workload="narrow-band 100x8 OERM, 64^3 channel, 3 levels 64/32/16 maxs 5/5/1e5, photmax %d, "
-                             "nVar 4, srt 1, calcwalls (adiabatic west wall)" % p.photmax,
-                    grid=[64, 64, 64], bands=100, gpoints=8, temps=64, photmax=p.photmax, nVar=4, levels=3)
     elif name == "grey32":
         p = W.config_grey_32(photmax=photmax or 64)
         tabs = None
-        desc = dict(workload="grey OERM kappa=1, 32^3 channel, photmax 64, nVar 4", grid=[32, 32, 32], photmax=64,
-                    nVar=4, levels=1)
     else:
         raise SystemExit("unknown workload " + name)
-    T = W.channel_field(p)
-    return p, tabs, T, desc
+    return p, tabs, W.channel_field(p), workload_desc(name, p)
+
+
+def workload_oracle(name, photmax=0):
+    """The same inputs built by the oracle alone (the reference arm never
+    loads the product library); tests/test_cpu_oracle_workload.py checks
+    they are identical byte for byte."""
+    from oracle import workload as OW
+    if name == "nb64":
+        p = OW.params_nb64(photmax=photmax or 256)
+        tabs = OW.tables_nb()
+    elif name == "grey32":
+        p = OW.channel_params(32, 32, 32, grey=True, photmax=photmax or 64)
+        tabs = None
+    else:
+        raise SystemExit("unknown workload " + name)
+    return p, tabs, OW.channel_field(p), workload_desc(name, p)
 
 
 class ClockSampler:
@@ -190,10 +222,72 @@ def cpu_sample(p, tabs, T, seconds=12.0, nthreads=0):
     return dict(bundles=r["bundles"], steps=r["steps"], seconds=dt, cells=n)
 
 
+def ref_cuda_child(lib_path, out_path, photmax):
+    """One solve of the reference's own CUDA build (oracle/_ref, built by
+    oracle/ref_build.py) in this process: tables written in its file formats
+    to a scratch directory (readT reads ./properties on every call), then
+    mc_gpu_ + get_results_ timed by oracle/ref_driver.cu."""
+    import ctypes as C
+    import tempfile
+
+    from oracle import workload as OW
+    p, tabs, T, _ = workload_oracle("nb64", photmax)
+    wd = tempfile.mkdtemp(prefix="rc_refcuda_")
+    OW.write_reference_dir(tabs, os.path.join(wd, "properties"))
+    os.chdir(wd)
+    lib = C.CDLL(lib_path)
+    fp = C.POINTER(C.c_float)
+    lib.ref_solve_timed.restype = C.c_int
+    lib.ref_solve_timed.argtypes = [fp, C.c_int, fp, fp, C.POINTER(C.c_double)]
+    shape = (p.kmax + 2, p.jmax + 2, p.imax + 2)
+    Q = np.zeros(shape, np.float32)
+    S = np.zeros(shape, np.float32)
+    ms = (C.c_double * 4)()
+    Tc = np.ascontiguousarray(T)
+    rc = lib.ref_solve_timed(Tc.ctypes.data_as(fp), 1, Q.ctypes.data_as(fp), S.ctypes.data_as(fp), ms)
+    with open(out_path, "w") as f:
+        json.dump({"rc": rc, "ms": list(ms), "finite": bool(np.isfinite(Q).all())}, f)
+
+
+def leg_ref_cuda(photmax, runs=3):
+    """The reference's own CUDA build of the workload (srt 1 as configured)
+    on this GPU: each solve in a child process of its own, because
+    get_results_ resets the device.  Reported: wall time of mc_gpu_ +
+    get_results_ and its parts (mc_gpu_ itself: table files, uploads,
+    launches; the kernels still running after it returns; get_results_),
+    and bundles/s on the wall clock and on the kernel time."""
+    import tempfile
+    lib = os.path.join(ROOT, "oracle", "_ref", "libref_nb64.so")
+    if not os.path.exists(lib):
+        return {"unavailable": "oracle/_ref/libref_nb64.so not built (the reference sources were absent at build)"}
+    out = []
+    for r in range(runs):
+        path = os.path.join(tempfile.mkdtemp(prefix="rc_refcuda_"), "r.json")
+        cp = subprocess.run([sys.executable, os.path.abspath(__file__), "--ref-cuda-child", lib, path,
+                             str(photmax)], capture_output=True, text=True, timeout=600)
+        if cp.returncode != 0 or not os.path.exists(path):
+            return {"unavailable": "reference CUDA build failed: " + (cp.stderr or cp.stdout)[-300:]}
+        out.append(json.load(open(path)))
+    ms = np.array([o["ms"] for o in out])
+    med = np.median(ms, axis=0)
+    bundles = 64 * 64 * 64 * 4 * photmax + 64 * 64 * 4 * photmax   # fluid cells + west-wall cells
+    return {"build": "oracle/_ref/libref_nb64.so (reference sources, srt 1 as configured, sm_100a)",
+            "runs": runs, "rc": [o["rc"] for o in out], "finite": all(o["finite"] for o in out),
+            "ms_wall": float(med[0]), "ms_mc_gpu": float(med[1]), "ms_kernels_after_return": float(med[2]),
+            "ms_get_results": float(med[3]), "ms_wall_runs": [float(x) for x in ms[:, 0]],
+            "bundles_per_solve": bundles, "bundles_per_s_wall": bundles / (med[0] / 1000.0),
+            "bundles_per_s_kernels": bundles / (med[2] / 1000.0),
+            "note": "kernels_after_return is the time from mc_gpu_'s return (kernels launched) to device idle"}
+
+
 def run_reference(args, ws, rank):
+    """The reference arm: the CPU restatement of the reference's ray loop
+    (the reference has no CPU implementation of this path) on all host cores,
+    on inputs the oracle builds itself; then the reference's own CUDA build
+    on this GPU (ref_cuda), outside the timed region."""
     if rank != 0:
         return
-    p, tabs, T, desc = workload(args.workload, args.photmax)
+    p, tabs, T, desc = workload_oracle(args.workload, args.photmax)
     cores = os.cpu_count() or 1
     for _ in range(args.warmup):
         cpu_sample(p, tabs, T, seconds=1.0)
@@ -211,10 +305,12 @@ def run_reference(args, ws, rank):
     line = {"impl": "reference", "metric": BUNDLE_METRIC, "value": v, "unit": "bundles/s", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * tot_t / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": dict(desc, parallelism="replicas"),
+            "config": bench_config(desc, ws),
             "steps_per_s": tot_s / tot_t,
             "cpu_baseline": {"value": v, "unit": "bundles/s", "cores": cores, "kind": "port", "sample": sample},
             "e2e": {"value": v, "unit": "bundles/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    if args.workload == "nb64" and not args.no_legs:
+        line["ref_cuda"] = leg_ref_cuda(p.photmax)
     print(json.dumps(line), flush=True)
 
 
@@ -635,7 +731,7 @@ def run_ours(args, ws, rank, local):
     line = {"metric": BUNDLE_METRIC, "value": value, "unit": "bundles/s", "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": 1000 * t_max / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": dict(desc, parallelism="replicas" if ws > 1 else "single", l2="flushed between steps"),
+            "config": bench_config(desc, ws),
             "steps_per_s": steps * ws / t_max, "solves_per_s": args.steps * ws / t_max,
             "rel_std_maxq": rel_std, "march_ms": 1000 * march_s / args.steps,
             "roofline": roof, "e2e": e2e, "gpu_launches": kernels_per_solve * args.steps,
@@ -685,7 +781,13 @@ def main():
     ap.add_argument("--serve-inflight", dest="serve_inflight", type=int, default=32)
     ap.add_argument("--policy", default="srpt", choices=["srpt", "fair"])
     ap.add_argument("--load", type=float, default=0.8)
+    ap.add_argument("--ref-cuda-child", dest="ref_cuda_child", nargs=3, default=None,
+                    help=argparse.SUPPRESS)
     args = ap.parse_args()
+    if args.ref_cuda_child:
+        lib, out, ph = args.ref_cuda_child
+        ref_cuda_child(lib, out, int(ph))
+        return
     ws, rank, local = dist_init()
     if args.serve:
         run_serve(args, rank, local)

@@ -251,7 +251,13 @@ int rc_autotune(rc_ctx *ctx, const float *T, int zstart, int pilot_photmax,
  * call on each device (make that first call before any stream capture) and
  * keeps its contents between calls; every element a solve reads is written
  * by the same solve first.  All calls in the process share the one array,
- * so calls that overlap on the GPU (several contexts or threads) race. */
+ * so calls that overlap on the GPU (several contexts or threads) race.
+ * qw64/vw64 rows of a wall whose flux is not computed are set to 0.  With
+ * no ticket to read rc_solve_info from, the solve's status word is reported
+ * by the return code: RC_E_RANGE, with the outputs written, when T was not
+ * finite (status bit 1), an index was out of bounds (bit 3, bounds-checked
+ * build; the message names the site) or T lay outside the table range
+ * (bit 0, end rows used); rc_last_error says which. */
 int rc_solve_noalloc(rc_ctx *ctx, const float *T_dev, int zstart, double *q64_dev, double *var64_dev,
                      double *qw64_dev, double *vw64_dev);
 int rc_destroy(rc_ctx *ctx);
@@ -287,6 +293,14 @@ typedef struct rc_trace_rec {
  * (level, ic, jc, kc) of the first max_cells steps of each bundle. */
 int rc_trace(rc_ctx *ctx, rc_ticket ticket, int n, const rc_bundle_id *ids,
              rc_trace_rec *out, int max_cells, int *cells);
+/* Band and g point that emission of the ticket's solve selects for
+ * caller-given uniforms u_band[n], u_g[n] (no counterpart in the reference;
+ * it exposes find_band / find_bandS, mc_gpu_noint.cu:1103-1233, for checks
+ * of their edge rules: u < cdf[0] -> 0, u == 1 -> last).  kind 0 searches
+ * the fluid band CDF at the table row nearest Tmax and the g CDF of that
+ * band, kind 1 or 2 the wall band CDF and the g weights' CDF. */
+int rc_sample_bands(rc_ctx *ctx, rc_ticket ticket, int kind, int n, const float *u_band,
+                    const float *u_g, int *nb, int *g);
 
 /* ---------------- batched solves ---------------- */
 

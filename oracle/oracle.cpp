@@ -140,6 +140,27 @@ int find_idx(const R *cdf, int n, R u) {
     return std::min(lo, n - 1);
 }
 
+// Wall band search edge rule.  0 (default): R below the wall CDF's own
+// first entry selects band 0.  1: the reference's find_bandS test against
+// the FLUID CDF's first entry probd[..][0] (mc_gpu_noint.cu:1189,1208), a
+// defect this solver does not reproduce; the oracle offers it so the
+// parity tests can measure what the defect does to the wall fluxes.
+int g_ref_wall_edge = 0;
+
+template <typename R>
+int find_idx_edge(const R *cdf, int n, R u, R edge0) {
+    int lo = 0, w = n;
+    while (w > lo + 1) {
+        int d = (lo + w) / 2;
+        if (u < cdf[d]) w = d;
+        if (u >= cdf[d]) lo = d;
+    }
+    lo = lo + 1;
+    if (u < edge0) lo = 0;
+    if (u == (R)1) lo = n - 1;
+    return std::min(lo, n - 1);
+}
+
 struct TraceSink {
     int max_cells = 0;
     int *cells = nullptr;
@@ -585,7 +606,7 @@ struct Problem {
             ray.ic = bound == 0 ? 1 : p.imax;
             ray.jc = j;
             ray.kc = k;
-            nb = find_idx(cdf_s.data(), nB, u_b);
+            nb = g_ref_wall_edge ? find_idx_edge(cdf_s.data(), nB, u_b, cdf_f[0]) : find_idx(cdf_s.data(), nB, u_b);
             g = (nQ > 1) ? find_idx(probq.data(), nQ, u_g) : 0;
             Ti = Tw0[bound][(size_t)(k - 1) * p.jmax + (j - 1)];
             Ibmax = Ibmax_w[bound];
@@ -830,6 +851,38 @@ int oracle_setup_scalars(const rc_params *p, const rc_tables *t, const float *T,
     return rc;
 }
 
+// Band and g point of emission for given uniforms (find_band / find_bandS,
+// mc_gpu_noint.cu:1103-1233, with the edge rule chosen by
+// oracle_set_ref_wall_edge for walls), and the CDF rows they search:
+// cdf_f / cdf_s [nB] (fluid / wall band CDF at the table row nearest
+// Tmax), probq [nQ]; any output may be NULL.
+int oracle_sample_bands(const rc_params *p, const rc_tables *t, const float *T, int kind, int n, const float *u_b,
+                        const float *u_g, int *nb, int *g, float *cdf_f, float *cdf_s, float *probq, int *row) {
+    if (!p || !T || kind < 0 || kind > 2) return RC_E_INVALID;
+    Problem<float> P;
+    int rc = P.init(*p, t, T);
+    if (rc) return rc;
+    const int nB = P.nB, nQ = P.nQ;
+    for (int i = 0; i < n; ++i) {
+        int b, q;
+        if (kind == 0) {
+            b = find_idx(P.cdf_f.data(), nB, u_b[i]);
+            q = nQ > 1 ? find_idx(&P.probg[((size_t)P.su.row * nB + b) * nQ], nQ, u_g[i]) : 0;
+        } else {
+            b = g_ref_wall_edge ? find_idx_edge(P.cdf_s.data(), nB, u_b[i], P.cdf_f[0])
+                                : find_idx(P.cdf_s.data(), nB, u_b[i]);
+            q = nQ > 1 ? find_idx(P.probq.data(), nQ, u_g[i]) : 0;
+        }
+        nb[i] = b;
+        g[i] = q;
+    }
+    if (cdf_f) memcpy(cdf_f, P.cdf_f.data(), nB * sizeof(float));
+    if (cdf_s && !P.cdf_s.empty()) memcpy(cdf_s, P.cdf_s.data(), nB * sizeof(float));
+    if (probq) memcpy(probq, P.probq.data(), nQ * sizeof(float));
+    if (row) *row = P.su.row;
+    return RC_OK;
+}
+
 int oracle_grid_level(const rc_params *p, int level, float *xu, float *yu, float *zu, float *x, float *y, float *z) {
     if (!p || level < 0 || level >= p->grid_num) return RC_E_INVALID;
     Grid g;
@@ -890,4 +943,119 @@ extern "C" int oracle_philox(const unsigned int *ctr, const unsigned int *key, u
     out[2] = r.z;
     out[3] = r.w;
     return RC_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Seeded synthetic correlated-k tables, restated from the table recipe of the
+// benchmark configurations so that the oracle's inputs need nothing from the
+// product library:
+//   k_{b,g}(T) = k0_b exp(kexp xi_g) (T/1000)^{n_b},
+//   log10 k0_b ~ U[logk_lo, logk_hi], n_b ~ U[-nexp, nexp] (Philox draws),
+//   xi_g / w_g the nQ-point Gauss-Legendre rule on [-1, 1] (w_g/2 as g
+//   weights), band centres ~ U[nu_lo, nu_hi] sorted with edges at midpoints,
+//   nT uniformly spaced temperatures on [T_lo, T_hi];
+//   band CDF ~ sum_g w_g k I_b dnu and g CDF ~ w_g k (nbcorrk/calc_prob.cpp
+//   :404-453), Planck mean pi sum k I_b dnu / (sigma T^4), and k_avg of the
+//   last temperature row (read_tables.cpp:52 overwrites it per row).
+// Outputs: caller arrays in the rc_tables layout (kq [nB][nT][nQ], prob
+// [nT][nB], probg [nT][nB][nQ]).
+// ---------------------------------------------------------------------------
+namespace {
+double draw_u53(uint64_t seed, uint32_t stream, uint32_t idx) {
+    rc_u32x4 c = {idx, stream, 0x5eedu, 0u};
+    const rc_u32x4 r = rc_philox4x32_10(c, (uint32_t)seed, (uint32_t)(seed >> 32));
+    const uint64_t hi = r.x >> 5, lo = r.y >> 6;  // 27 + 26 bits
+    return (double)(hi * 67108864ull + lo) * (1.0 / 9007199254740992.0);
+}
+
+// Gauss-Legendre nodes (ascending) and weights by Newton's method on P_n.
+void gl_rule(int n, std::vector<double> &x, std::vector<double> &w) {
+    x.assign(n, 0.0);
+    w.assign(n, 0.0);
+    for (int i = 0; i < n; ++i) {
+        double z = cos(RC_PI_D * (i + 0.75) / (n + 0.5)), dp = 0.0;
+        for (int it = 0; it < 100; ++it) {
+            double p1 = 1.0, p2 = 0.0;
+            for (int j = 1; j <= n; ++j) {
+                const double p3 = p2;
+                p2 = p1;
+                p1 = ((2.0 * j - 1.0) * z * p2 - (j - 1.0) * p3) / j;
+            }
+            dp = n * (z * p1 - p2) / (z * z - 1.0);
+            const double z0 = z;
+            z = z0 - p1 / dp;
+            if (fabs(z - z0) < 1e-15) break;
+        }
+        x[n - 1 - i] = z;
+        w[n - 1 - i] = 2.0 / ((1.0 - z * z) * dp * dp);
+    }
+}
+}  // namespace
+
+extern "C" int oracle_set_ref_wall_edge(int on) {
+    g_ref_wall_edge = on ? 1 : 0;
+    return 0;
+}
+
+extern "C" int oracle_tables_synthetic(const rc_synth_spec *s, float *Tnb, float *kP, float *wvl, float *wvr,
+                                       float *wvc, float *kavg, float *kq, float *prob, float *probg, float *wq) {
+    if (!s || s->nB < 1 || s->nQ < 1 || s->nT < 2 || !(s->T_hi > s->T_lo) || !(s->T_lo > 0) ||
+        !(s->nu_hi > s->nu_lo) || !(s->nu_lo > 0))
+        return -1;
+    const int nB = s->nB, nQ = s->nQ, nT = s->nT;
+    std::vector<double> xi, wgl;
+    gl_rule(nQ, xi, wgl);
+    std::vector<double> wg(nQ);
+    for (int g = 0; g < nQ; ++g) {
+        wg[g] = wgl[g] / 2.0;
+        wq[g] = (float)wg[g];
+    }
+    std::vector<double> nu(nB), k0(nB), ne(nB), el(nB), er(nB);
+    for (int b = 0; b < nB; ++b) nu[b] = s->nu_lo + (s->nu_hi - s->nu_lo) * draw_u53(s->seed, 1, b);
+    std::sort(nu.begin(), nu.end());
+    for (int b = 0; b < nB; ++b) {
+        k0[b] = pow(10.0, s->logk_lo + (s->logk_hi - s->logk_lo) * draw_u53(s->seed, 2, b));
+        ne[b] = -s->nexp + 2.0 * s->nexp * draw_u53(s->seed, 3, b);
+    }
+    for (int b = 0; b < nB; ++b) {
+        el[b] = b == 0 ? s->nu_lo : 0.5 * (nu[b - 1] + nu[b]);
+        er[b] = b == nB - 1 ? s->nu_hi : 0.5 * (nu[b] + nu[b + 1]);
+        wvl[b] = (float)el[b];
+        wvr[b] = (float)er[b];
+        wvc[b] = (float)nu[b];
+    }
+    const double sigma = 5.670373e-08;
+    std::vector<double> kg(nQ), pband(nB);
+    for (int i = 0; i < nT; ++i) {
+        const double T = s->T_lo + (s->T_hi - s->T_lo) * i / (double)(nT - 1);
+        Tnb[i] = (float)T;
+        double total = 0.0;
+        for (int b = 0; b < nB; ++b) {
+            const double ib = rc_planck(T, nu[b]);
+            const double dnu = (er[b] - el[b]) * 100.0;
+            double kav = 0.0, pb = 0.0, sg = 0.0;
+            for (int g = 0; g < nQ; ++g) {
+                kg[g] = k0[b] * exp(s->kexp * xi[g]) * pow(T / 1000.0, ne[b]);
+                kq[((size_t)b * nT + i) * nQ + g] = (float)kg[g];
+                kav += wg[g] * kg[g];
+                pb += wg[g] * kg[g] * ib * dnu;
+            }
+            if (i == nT - 1) kavg[b] = (float)kav;
+            pband[b] = pb;
+            total += pb;
+            for (int g = 0; g < nQ; ++g) sg += kg[g] * wg[g];
+            double cg = 0.0;
+            for (int g = 0; g < nQ; ++g) {
+                cg += kg[g] * wg[g];
+                probg[((size_t)i * nB + b) * nQ + g] = g == nQ - 1 ? 1.0f : (float)(cg / sg);
+            }
+        }
+        kP[i] = (float)(RC_PI_D * total / (sigma * T * T * T * T));
+        double c = 0.0;
+        for (int b = 0; b < nB; ++b) {
+            c += pband[b];
+            prob[(size_t)i * nB + b] = b == nB - 1 ? 1.0f : (float)(c / total);
+        }
+    }
+    return 0;
 }

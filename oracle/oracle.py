@@ -1,7 +1,8 @@
 """ctypes bindings of the CPU oracle (oracle/_build/liboracle.so).
 
 TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and
-bench.py's CPU baseline, never by the product package.
+bench.py's CPU legs, never by the product package.  It does not import the
+product package either: the C structures come from oracle/abi.py.
 """
 from __future__ import annotations
 
@@ -10,7 +11,7 @@ import os
 
 import numpy as np
 
-from radchan_b200 import _lib as L
+from oracle import abi as L
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "_build", "liboracle.so")
@@ -61,7 +62,11 @@ def _dp(a):
 
 
 def _tv(tables):
-    return C.byref(tables.view) if tables is not None else None
+    return C.byref(L.tables_view(tables.view)) if tables is not None else None
+
+
+def _pp(p):
+    return C.byref(L.params(p))
 
 
 def solve(p, tables, T, zstart=1, rpt=8, cell_begin=0, cell_end=-1, walls=True, fp64=False, nthreads=0):
@@ -73,7 +78,7 @@ def solve(p, tables, T, zstart=1, rpt=8, cell_begin=0, cell_end=-1, walls=True, 
     vw = np.zeros((2, kl, p.jmax))
     st = C.c_double()
     nb = C.c_double()
-    rc = lib().oracle_solve(C.byref(p), _tv(tables), _fp(T), zstart, rpt, cell_begin, cell_end, 1 if walls else 0,
+    rc = lib().oracle_solve(_pp(p), _tv(tables), _fp(T), zstart, rpt, cell_begin, cell_end, 1 if walls else 0,
                             1 if fp64 else 0, nthreads, _dp(q), _dp(v), _dp(qw), _dp(vw), C.byref(st), C.byref(nb))
     if rc != 0:
         raise RuntimeError("oracle_solve failed: %d" % rc)
@@ -86,7 +91,7 @@ def trace(p, tables, T, ids, max_cells=0, fp64=False):
     arr = (L.RcBundleId * n)(*[L.RcBundleId(*b) for b in ids])
     out = (L.RcTraceRec * n)()
     cells = np.full((n, max(max_cells, 1), 4), -1, np.int32)
-    rc = lib().oracle_trace(C.byref(p), _tv(tables), _fp(T), 1, 1 if fp64 else 0, n, arr, out, max_cells,
+    rc = lib().oracle_trace(_pp(p), _tv(tables), _fp(T), 1, 1 if fp64 else 0, n, arr, out, max_cells,
                             cells.ctypes.data_as(C.POINTER(C.c_int)) if max_cells > 0 else None)
     if rc != 0:
         raise RuntimeError("oracle_trace failed: %d" % rc)
@@ -96,7 +101,7 @@ def trace(p, tables, T, ids, max_cells=0, fp64=False):
 def setup(p, tables, T, fp64=False):
     T = np.ascontiguousarray(T, dtype=np.float32)
     s = OracleSetup()
-    rc = lib().oracle_setup_scalars(C.byref(p), _tv(tables), _fp(T), 1 if fp64 else 0, C.byref(s))
+    rc = lib().oracle_setup_scalars(_pp(p), _tv(tables), _fp(T), 1 if fp64 else 0, C.byref(s))
     if rc != 0:
         raise RuntimeError("oracle_setup_scalars failed: %d" % rc)
     return s
@@ -106,7 +111,7 @@ def grid_level(p, level=0):
     im, jm, km = p.maxi[level], p.maxj[level], p.maxk[level]
     a = {n: np.zeros(s, np.float32) for n, s in
          (("xu", im + 1), ("yu", jm + 1), ("zu", km + 1), ("x", im + 2), ("y", jm + 2), ("z", km + 2))}
-    rc = lib().oracle_grid_level(C.byref(p), level, _fp(a["xu"]), _fp(a["yu"]), _fp(a["zu"]), _fp(a["x"]),
+    rc = lib().oracle_grid_level(_pp(p), level, _fp(a["xu"]), _fp(a["yu"]), _fp(a["zu"]), _fp(a["x"]),
                                  _fp(a["y"]), _fp(a["z"]))
     if rc != 0:
         raise RuntimeError("oracle_grid_level failed")
@@ -116,7 +121,39 @@ def grid_level(p, level=0):
 def level_T(p, T, level):
     T = np.ascontiguousarray(T, dtype=np.float32)
     out = np.zeros((p.maxk[level], p.maxj[level], p.maxi[level]), np.float32)
-    rc = lib().oracle_level_T(C.byref(p), _fp(T), level, _fp(out))
+    rc = lib().oracle_level_T(_pp(p), _fp(T), level, _fp(out))
     if rc != 0:
         raise RuntimeError("oracle_level_T failed")
     return out
+
+
+def sample_bands(p, tables, T, kind, u_b, u_g, ref_wall_edge=False):
+    """Band and g point of emission for given uniforms, and the CDF rows
+    searched: (nb, g, cdf_f, cdf_s, probq, row)."""
+    T = np.ascontiguousarray(T, dtype=np.float32)
+    ub = np.ascontiguousarray(u_b, np.float32)
+    ug = np.ascontiguousarray(u_g, np.float32)
+    n = ub.size
+    nb = np.zeros(n, np.int32)
+    g = np.zeros(n, np.int32)
+    nB = 1000 if p.grey else p.nB
+    nQ = 1 if p.grey else p.nQ
+    cf, cs, pq = np.zeros(max(nB, p.grey_nB), np.float32), np.zeros(max(nB, p.grey_nB), np.float32), np.zeros(
+        max(nQ, 1), np.float32)
+    row = C.c_int()
+    f = lib().oracle_sample_bands
+    f.restype = C.c_int
+    ip = lambda a: a.ctypes.data_as(C.POINTER(C.c_int))
+    f.argtypes = [C.POINTER(L.RcParams), C.POINTER(L.RcTables), C.POINTER(C.c_float), C.c_int, C.c_int,
+                  C.POINTER(C.c_float), C.POINTER(C.c_float), C.POINTER(C.c_int), C.POINTER(C.c_int),
+                  C.POINTER(C.c_float), C.POINTER(C.c_float), C.POINTER(C.c_float), C.POINTER(C.c_int)]
+    lib().oracle_set_ref_wall_edge(1 if ref_wall_edge else 0)
+    try:
+        rc = f(_pp(p), _tv(tables), _fp(T), kind, n, _fp(ub), _fp(ug), ip(nb), ip(g), _fp(cf), _fp(cs), _fp(pq),
+               C.byref(row))
+    finally:
+        lib().oracle_set_ref_wall_edge(0)
+    if rc != 0:
+        raise RuntimeError("oracle_sample_bands failed: %d" % rc)
+    nb_used = p.grey_nB if p.grey else p.nB
+    return nb, g, cf[:nb_used], cs[:nb_used], pq[:nQ], row.value

@@ -10,6 +10,20 @@ Recipe (nothing from the reference is copied into this repository):
      - the grey-gas table reader writes probg[nT][nB][nQ], one row past the end
        of a global array (read_tables.cpp:169-170); the patch writes
        probg[i][j][g] so no host memory outside the array is overwritten;
+     - kernel_surface hands march_ray an Emission it never fills
+       (mc_gpu_noint.cu:1330, "not going to be used since this is done only
+       for adiabatic walls"); a wall bundle that reaches the opposite x wall
+       when that wall is black and NOT adiabatic (the C2 case: adiabatic west
+       wall, black east wall at 573 K) deposits Ibmax*tra*(invTi4*emiss.east
+       - 1)*ratioI with emiss.east read from uninitialised memory
+       (mc_gpu_noint.cu:432-440), which made the wall fluxes NaN.  The patch
+       fills emiss from the wall spectra after the band draw exactly as
+       kernel_fluid does (mc_gpu_noint.cu:157-175), through a __device__
+       pointer to Ibw_d[gpu] set before the launch;
+     - only in the "nb64s0fix" build: find_bandS's edge rule tests the wall
+       CDF probs instead of the fluid CDF probd (mc_gpu_noint.cu:1189, :1208),
+       the defect this solver does not reproduce, so that the wall fluxes of
+       both solvers can be compared directly;
   3. rewrite the #define values of param.h (and the maxi/maxj/maxk initialisers)
      for the configuration; for the narrow-band configurations also nT/nQ/nB
      in NarrowBand.h and the constant g-CDF probq (mc_gpu_noint.cu:34-36,
@@ -33,7 +47,7 @@ import tempfile
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
-REF = "/root/reference"
+REF = os.environ.get("RADCHAN_REFERENCE", "/root/reference")
 OUT = os.path.join(HERE, "_ref")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 
@@ -65,10 +79,14 @@ _NB = dict(num_gpu="1", p_col="1", imax="64", jmax="64", kmax="64", Lx="2.f", Ly
            floatpoint="0", epsw="1.f", epse="1.f", epss="1.f", epsn="1.f", epsb="1.f", epst="1.f", Tww="955",
            Twe="573", Tws="0", Twn="0", Twb="0", Twt="0", adiabw="1", adiabe="0", toll="1.0e-3", tollS="1.0e-3",
            bdw="2", bde="2", bds="1", bdn="1", bdb="1", bdt="1")
-for _name, _srt in (("nb64", "1"), ("nb64s0", "0")):
+for _name, _srt in (("nb64", "1"), ("nb64s0", "0"), ("nb64s0fix", "0")):
     CONFIGS[_name] = dict(defines=dict(_NB, srt=_srt), levels=["imax", "imax/2", "imax/4"],
                           levels_j=["jmax", "jmax/2", "jmax/4"], levels_k=["kmax", "kmax/2", "kmax/4"],
                           narrowband=dict(nT="64", nQ="8", nB="100"))
+# "nb64s0fix" also corrects find_bandS's edge rule (see _patch_wall_edge), so
+# that the wall fluxes can be compared with a solver that does not carry the
+# defect; "nb64s0" keeps it.
+CONFIGS["nb64s0fix"]["wall_edge_fix"] = True
 
 
 def _patch_mc(src: str) -> str:
@@ -88,7 +106,60 @@ def _patch_mc(src: str) -> str:
         "  cudaMemcpyToSymbol(rc_tex_Ib_obj, &to, sizeof(to)); }", src)
     if "#include <string.h>" not in src:
         src = "#include <string.h>\n" + src
+    return _patch_surface_emission(src)
+
+
+_SURF_FILL = """
+#if adiabw == 0
+					emiss.west  = rc_Ibw_ptr->west[nb];
+#endif
+#if adiabe == 0
+					emiss.east  = rc_Ibw_ptr->east[nb];
+#endif
+#if bdt != 1
+					emiss.top   = rc_Ibw_ptr->top[nb];
+#endif
+#if bdb != 1
+					emiss.bot   = rc_Ibw_ptr->bot[nb];
+#endif
+#if bdn != 1
+					emiss.north = rc_Ibw_ptr->north[nb];
+#endif
+#if bds != 1
+					emiss.south = rc_Ibw_ptr->south[nb];
+#endif
+"""
+
+
+def _patch_surface_emission(src: str) -> str:
+    """kernel_surface: fill the Emission handed to march_ray from the wall
+    spectra (mc_gpu_noint.cu:1330, :1418; kernel_fluid's rule :157-175)."""
+    decl = "__device__ cudaTextureObject_t rc_tex_Ib_obj;"
+    assert decl in src
+    src = src.replace(decl, decl + "\n__device__ EmissSpec *rc_Ibw_ptr;", 1)
+    k = src.index("__global__ void kernel_surface(")
+    band = "\t\t\t\t\twvc  \t= wvc_d[nb];\n"
+    j = src.index(band, k)
+    src = src[:j + len(band)] + _SURF_FILL + src[j + len(band):]
+    launch = "\t\t\tkernel_surface<<<"
+    assert src.count(launch) == 1
+    src = src.replace(launch, "\t\t\tcudaMemcpyToSymbol(rc_Ibw_ptr, &Ibw_d[gpu], sizeof(EmissSpec *));\n" + launch, 1)
     return src
+
+
+def _patch_wall_edge(src: str) -> str:
+    """find_bandS bisects the wall CDF probs but applies the R < cdf[0]
+    edge rule to the fluid CDF probd (mc_gpu_noint.cu:1189, :1208): uniforms
+    between probd[t][0] and probs[t][0] select band 1 instead of band 0.
+    The patch tests probs[t-tm][0] in both branches."""
+    k = src.index("__device__ __forceinline__ void find_bandS(")
+    end = src.index("__device__ __forceinline__ void wave_find(", k)
+    body = src[k:end]
+    old = "if( Rwave <  probd[t-tm][0] )"
+    old2 = "if(Rwave <  probd[t-tm][0] )"
+    assert body.count(old) == 1 and body.count(old2) == 1
+    body = body.replace(old, "if( Rwave <  probs[t-tm][0] )").replace(old2, "if(Rwave <  probs[t-tm][0] )")
+    return src[:k] + body + src[end:]
 
 
 def _patch_tables(src: str) -> str:
@@ -153,6 +224,8 @@ def build(name: str, verbose: bool = False) -> str:
         patches = [(os.path.join(mc, "mc_gpu_noint.cu"), _patch_mc),
                    (os.path.join(mc, "read_tables.cpp"), _patch_tables),
                    (os.path.join(pa, "param.h"), lambda t: _patch_param(t, cfg))]
+        if cfg.get("wall_edge_fix"):
+            patches.append((os.path.join(mc, "mc_gpu_noint.cu"), _patch_wall_edge))
         if "narrowband" in cfg:
             wq = _table_wq()
             patches.append((os.path.join(mc, "mc_gpu_noint.cu"), lambda t: _patch_probq(t, wq)))
@@ -195,7 +268,8 @@ def build_if_present() -> None:
         return
     for name in CONFIGS:
         lib = os.path.join(OUT, "libref_%s.so" % name)
-        if not os.path.exists(lib) or os.path.getmtime(lib) < os.path.getmtime(__file__):
+        newest = max(os.path.getmtime(__file__), os.path.getmtime(os.path.join(HERE, "ref_driver.cu")))
+        if not os.path.exists(lib) or os.path.getmtime(lib) < newest:
             build(name)
 
 

@@ -329,6 +329,19 @@ class Solver:
                                  cells.ctypes.data_as(C.POINTER(C.c_int)) if max_cells > 0 else None), self.ctx)
         return list(out), cells[:, :max_cells]
 
+    def sample_bands(self, ticket, kind, u_band, u_g):
+        """Band and g point that emission selects for the given uniforms
+        (rc_sample_bands)."""
+        ub = np.ascontiguousarray(u_band, np.float32)
+        ug = np.ascontiguousarray(u_g, np.float32)
+        assert ub.shape == ug.shape and ub.ndim == 1
+        nb = np.zeros(ub.size, np.int32)
+        g = np.zeros(ub.size, np.int32)
+        ip = lambda a: a.ctypes.data_as(C.POINTER(C.c_int))
+        fp = lambda a: a.ctypes.data_as(C.POINTER(C.c_float))
+        L.check(L.lib().rc_sample_bands(self.ctx, ticket, kind, ub.size, fp(ub), fp(ug), ip(nb), ip(g)), self.ctx)
+        return nb, g
+
     def autotune(self, T, zstart=1, pilot_photmax=16):
         """Pick rays_per_thread, block_threads, sort_bands and occupancy by
         timing pilot solves on T; returns the chosen (rpt, block, sort, occupancy)."""

@@ -262,6 +262,26 @@ __device__ __forceinline__ int guided_index(const R *cdf, const int *guide, int 
     return u == (R)1 ? n - 1 : b;
 }
 
+// Band and g point of an emitted bundle from its two uniforms: fluid bundles
+// (kind 0) search the band CDF at the table row nearest Tmax and then the
+// g CDF of that band and row (find_band, mc_gpu_noint.cu:1103-1169); wall
+// bundles (kind 1, 2) the Planck-only wall band CDF and the constant g CDF
+// probq (find_bandS :1170-1233, with the wall CDF's own edge rule).
+template <typename R>
+__device__ __forceinline__ void select_band_g(const DSolve<R> &S, int kind, R u_b, R u_g, int &nb, int &g) {
+    if (kind == 0) {
+        nb = (int)RC_IX(guided_index(S.cdf_f, S.guide_f, S.nB, u_b), S.nB, SITE_CDF, S);
+        g = (S.nQ > 1)
+                ? bisect(S.probg + RC_IX(((size_t)S.row * S.nB + nb) * S.nQ, (long long)S.nT * S.nB * S.nQ,
+                                         SITE_PROBG, S),
+                         S.nQ, u_g)
+                : 0;
+    } else {
+        nb = (int)RC_IX(guided_index(S.cdf_s, S.guide_s, S.nB, u_b), S.nB, SITE_CDF, S);
+        g = (S.nQ > 1) ? bisect(S.probq, S.nQ, u_g) : 0;
+    }
+}
+
 // A bundle after emission, placed at its start point: position, cell,
 // direction, sampled band/g and OERM weights.
 template <typename R>
@@ -326,12 +346,7 @@ __device__ __forceinline__ bool emit_bundle(Emitted<R> &e, const DSolve<R> &S, i
         const R mu = (R)1 - (R)2 * u_mu;
         st = RT<R>::sqrt_(((R)1 - mu) * ((R)1 + mu));
         e.sx = mu;
-        nb = (int)RC_IX(guided_index(S.cdf_f, S.guide_f, S.nB, u_b), S.nB, SITE_CDF, S);
-        g = (S.nQ > 1)
-                ? bisect(S.probg + RC_IX(((size_t)S.row * S.nB + nb) * S.nQ, (long long)S.nT * S.nB * S.nQ,
-                                         SITE_PROBG, S),
-                         S.nQ, u_g)
-                : 0;
+        select_band_g(S, 0, u_b, u_g, nb, g);
         const DLevel<R> &L0 = S.lev[0];
         Pi = L0.P[RC_IX(cell_index(i, j, k, L0.im, L0.jm), (long long)L0.im * L0.jm * L0.km, SITE_EMIT_T, S)];
         e.xp = S.xc[RC_IX(i, S.imax + 2, SITE_CENTRE, S)];
@@ -346,8 +361,7 @@ __device__ __forceinline__ bool emit_bundle(Emitted<R> &e, const DSolve<R> &S, i
             e.sx = -RT<R>::sqrt_(u_mu);
             st = RT<R>::sqrt_((R)1 - u_mu);
         }
-        nb = (int)RC_IX(guided_index(S.cdf_s, S.guide_s, S.nB, u_b), S.nB, SITE_CDF, S);
-        g = (S.nQ > 1) ? bisect(S.probq, S.nQ, u_g) : 0;
+        select_band_g(S, kind, u_b, u_g, nb, g);
         Pi = S.Pw0[bound][RC_IX((k - 1) * S.jmax + (j - 1), (long long)S.kmax * S.jmax, SITE_WALL_EMIT_T, S)];
         ic = (bound == 0) ? 1 : S.imax;
         e.xp = (bound == 0) ? (R)0 : S.Lx;

@@ -1230,6 +1230,30 @@ struct Impl : ImplBase {
         if (d_cells) cudaFree(d_cells);
         return RC_OK;
     }
+
+    int sample_bands(rc_ticket t, int kind, int n, const float *u_b, const float *u_g, int *nb, int *g) {
+        std::string *err_ = &c->err;
+        Slot<R> *sp = find_slot(t);
+        if (!sp) return set_err(err_, RC_E_STATE, "unknown ticket");
+        int rc = wait(*sp);
+        if (rc) return rc;
+        if (kind < 0 || kind > 2) return set_err(err_, RC_E_INVALID, "kind must be 0 (fluid), 1 or 2 (walls)");
+        if (n <= 0) return RC_OK;
+        float *d_u = nullptr;
+        int *d_i = nullptr;
+        RC_CK(cudaMalloc((void **)&d_u, 2 * (size_t)n * sizeof(float)));
+        RC_CK(cudaMalloc((void **)&d_i, 2 * (size_t)n * sizeof(int)));
+        RC_CK(cudaMemcpy(d_u, u_b, n * sizeof(float), cudaMemcpyHostToDevice));
+        RC_CK(cudaMemcpy(d_u + n, u_g, n * sizeof(float), cudaMemcpyHostToDevice));
+        k_sample_bands<R><<<(n + 127) / 128, 128, 0, sp->st>>>(sp->d_desc, kind, n, d_u, d_u + n, d_i, d_i + n);
+        RC_CK(cudaGetLastError());
+        RC_CK(cudaStreamSynchronize(sp->st));
+        RC_CK(cudaMemcpy(nb, d_i, n * sizeof(int), cudaMemcpyDeviceToHost));
+        RC_CK(cudaMemcpy(g, d_i + n, n * sizeof(int), cudaMemcpyDeviceToHost));
+        cudaFree(d_u);
+        cudaFree(d_i);
+        return RC_OK;
+    }
 };
 
 // dispatch helpers

@@ -347,4 +347,18 @@ __global__ void k_trace(const DSolve<R> *Sp, int n, const rc_bundle_id *ids, rc_
     out[t] = rec;
 }
 
+// Band and g point that emission selects for caller-given uniforms (the
+// edge rules of the CDF searches, checked against the oracle and the
+// reference's bisection): the same select_band_g the march's emission uses.
+template <typename R>
+__global__ void k_sample_bands(const DSolve<R> *Sp, int kind, int n, const float *u_b, const float *u_g, int *nb,
+                               int *g) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    int b, q;
+    select_band_g(*Sp, kind, (R)u_b[t], (R)u_g[t], b, q);
+    nb[t] = b;
+    g[t] = q;
+}
+
 }  // namespace rc

@@ -37,33 +37,8 @@ void report(const char *what) {
     fprintf(stderr, "radchan: %s failed: %s\n", what, buf);
 }
 
-int configure_from_env() {
-    const char *ph = getenv("RADCHAN_PARAM_H");
-    if (!ph) {
-        fprintf(stderr, "radchan: mc_gpu_ called before rc_legacy_configure and RADCHAN_PARAM_H is not set\n");
-        return RC_E_STATE;
-    }
-    const char *nh = getenv("RADCHAN_NARROWBAND_H");
-    rc_params p;
-    int rc = rc_params_from_headers(ph, nh, &p);
-    if (rc) return rc;
-    if (p.grey) return rc_legacy_configure(&p, nullptr);
-    const char *dir = getenv("RADCHAN_PROPERTIES");
-    rc_table_set *ts = nullptr;
-    rc = rc_tables_read_dir(dir ? dir : "properties", p.nT, p.nB, p.nQ, &ts);
-    if (rc) return rc;
-    rc_tables v;
-    rc_tables_view(ts, &v);
-    rc = rc_legacy_configure(&p, &v);
-    rc_tables_free(ts);
-    return rc;
-}
-}  // namespace
-
-extern "C" {
-
-int rc_legacy_configure(const rc_params *p, const rc_tables *tables) {
-    std::lock_guard<std::mutex> lk(g_mu);
+// Replaces the process-wide context; the caller holds g_mu.
+int configure_locked(const rc_params *p, const rc_tables *tables) {
     if (g_ctx) {
         rc_destroy(g_ctx);
         g_ctx = nullptr;
@@ -87,6 +62,37 @@ int rc_legacy_configure(const rc_params *p, const rc_tables *tables) {
     return RC_OK;
 }
 
+// Configures the context from the environment; the caller holds g_mu.
+int configure_from_env() {
+    const char *ph = getenv("RADCHAN_PARAM_H");
+    if (!ph) {
+        fprintf(stderr, "radchan: mc_gpu_ called before rc_legacy_configure and RADCHAN_PARAM_H is not set\n");
+        return RC_E_STATE;
+    }
+    const char *nh = getenv("RADCHAN_NARROWBAND_H");
+    rc_params p;
+    int rc = rc_params_from_headers(ph, nh, &p);
+    if (rc) return rc;
+    if (p.grey) return configure_locked(&p, nullptr);
+    const char *dir = getenv("RADCHAN_PROPERTIES");
+    rc_table_set *ts = nullptr;
+    rc = rc_tables_read_dir(dir ? dir : "properties", p.nT, p.nB, p.nQ, &ts);
+    if (rc) return rc;
+    rc_tables v;
+    rc_tables_view(ts, &v);
+    rc = configure_locked(&p, &v);
+    rc_tables_free(ts);
+    return rc;
+}
+}  // namespace
+
+extern "C" {
+
+int rc_legacy_configure(const rc_params *p, const rc_tables *tables) {
+    std::lock_guard<std::mutex> lk(g_mu);
+    return configure_locked(p, tables);
+}
+
 int rc_legacy_release(void) {
     std::lock_guard<std::mutex> lk(g_mu);
     if (g_ctx) rc_destroy(g_ctx);
@@ -97,13 +103,15 @@ int rc_legacy_release(void) {
 
 void mc_gpu_(float *T, int *zstart, int *rank) {
     (void)rank;
+    std::lock_guard<std::mutex> lk(g_mu);
+    // the first call configures the context; under the lock, so that two
+    // first calls from different threads configure it once
     if (!g_ctx) {
         if (configure_from_env()) {
             report("mc_gpu_ configuration");
             return;
         }
     }
-    std::lock_guard<std::mutex> lk(g_mu);
     if (g_have_ticket) {
         // a previous launch was never collected: finish it first
         rc_collect(g_ctx, g_ticket, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr);

@@ -245,6 +245,14 @@ int rc_trace(rc_ctx *c, rc_ticket t, int n, const rc_bundle_id *ids, rc_trace_re
     return with_impl(c, [&](auto &im) { return im.trace(t, n, ids, out, max_cells, cells); });
 }
 
+int rc_sample_bands(rc_ctx *c, rc_ticket t, int kind, int n, const float *u_band, const float *u_g, int *nb,
+                    int *g) {
+    if (!c || (n > 0 && (!u_band || !u_g || !nb || !g)))
+        return set_err(c ? &c->err : nullptr, RC_E_INVALID, "NULL argument");
+    cudaSetDevice(c->device);
+    return with_impl(c, [&](auto &im) { return im.sample_bands(t, kind, n, u_band, u_g, nb, g); });
+}
+
 int rc_destroy(rc_ctx *c) {
     if (!c) return RC_OK;
     cudaSetDevice(c->device);
@@ -645,13 +653,31 @@ int solve_noalloc_t(rc_ctx *c, const float *T_dev, int zstart, double *q64, doub
     s.h_tiles[0] = 0;
     s.h_tiles[1] = s.h_desc->n_tiles;
     RC_CK(cudaMemcpyAsync(s.d_tiles, s.h_tiles, 2 * sizeof(long long), cudaMemcpyHostToDevice, st));
+    // The tally writes only the walls whose flux is computed; the others read
+    // 0, as the allocating entry points return them.
+    const int nwalls = s.h_desc->nwalls;
+    const size_t wall_bytes = 2 * (size_t)s.h_desc->nwc * sizeof(double);
+    if (nwalls < 2 && qw64) RC_CK(cudaMemsetAsync(qw64, 0, wall_bytes, st));
+    if (nwalls < 2 && vw64) RC_CK(cudaMemsetAsync(vw64, 0, wall_bytes, st));
     rc = im.launch_march(s.d_desc, s.d_tiles, 1, s.h_desc->n_tiles, s.d_counter, c->block, rpt, st);
     if (rc) return rc;
     rc = im.launch_tally(s.d_desc, s.d_out, 1, im.tally_cells(), st);
     if (rc) return rc;
     RC_CK(cudaMemcpyAsync(s.h_sc, s.d_sc, sizeof(DScalars), cudaMemcpyDeviceToHost, st));
     RC_CK(cudaStreamSynchronize(st));
-    if (s.h_sc->status & 2) return set_err(err_, RC_E_RANGE, "temperature field contains non-finite values");
+    // No ticket exists to read rc_solve_info from, so the status word of the
+    // solve travels in the return code and the message.  The outputs are
+    // written in every case below.
+    const int status = s.h_sc->status;
+    if (status & 2) return set_err(err_, RC_E_RANGE, "temperature field contains non-finite values (status bit 1)");
+    if (status & 8)
+        return set_err(err_, RC_E_RANGE,
+                       "an index was out of bounds in the march (status bit 3, bounds-checked build), first at site " +
+                           std::to_string(s.h_sc->bad_site));
+    if (status & 1)
+        return set_err(err_, RC_E_RANGE,
+                       "temperature outside the table range (status bit 0): results written with the end rows of "
+                       "the tables (clamped)");
     return RC_OK;
 }
 

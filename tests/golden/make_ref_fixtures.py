@@ -8,17 +8,22 @@ fixtures:
       temperature field, and the wall-clock times of mc_gpu_+get_results_.
   tests/golden/ref_nb64.npz    -- narrow-band 64^3 channel (100 bands x 8 g,
       64 temperatures of the seeded synthetic tables, 3 levels 64/32/16,
-      photmax 256, nVar 4, adiabatic west wall with its flux), built with
-      srt = 0 so that its replicates are independent: per-x-plane means of Q
-      and their standard errors, the mean west-wall flux and its standard
-      error, Q and sigma of 4096 sampled cells, and the wall-clock times of
-      the srt = 0 and srt = 1 (as configured) builds.
+      photmax 256, nVar 4, adiabatic west wall with its flux).  From the
+      srt = 0 build (independent replicates): per-x-plane means of Q and their
+      standard errors, Q and sigma of 4096 sampled cells, and the west-wall
+      flux and its sigma at every wall cell.  From the srt = 1 build (as the
+      configuration states; its replicates share one band histogram per
+      thread, so its sigma is biased low): per-x-plane means of Q with the
+      standard errors it reports, and its west-wall flux and sigma at every
+      wall cell.  From the srt = 0 build whose find_bandS edge rule is
+      corrected ("nb64s0fix", oracle/ref_build.py): the west-wall flux and
+      sigma at every wall cell.  Wall-clock times of the builds.
 
 The reference resets the device inside get_results_ and reads its tables
 from ./properties, so every solve runs in a child process of its own, in a
 scratch directory holding the table files.  Usage (on a GPU machine):
 
-    python tests/golden/make_ref_fixtures.py [--config grey32|nb64] [--repeats 3]
+    python tests/golden/make_ref_fixtures.py [--config grey32|nb64] [--repeats 3] [--outdir DIR]
 """
 from __future__ import annotations
 
@@ -91,6 +96,7 @@ def main():
     ap.add_argument("--lib", default=None)
     ap.add_argument("--out", default=None)
     ap.add_argument("--workdir", default=None)
+    ap.add_argument("--outdir", default=HERE, help="where the .npz fixture is written")
     a = ap.parse_args()
     if a.child:
         child(a.child, a.lib, a.out, a.workdir)
@@ -101,26 +107,41 @@ def main():
         Q = runs[0]["Q"][1:-1, 1:-1, 1:-1]
         S = runs[0]["sigma"][1:-1, 1:-1, 1:-1]
         meta = dict(config="grey32", field_seed=FIELD_SEED, ms=[float(r["ms"]) for r in runs], repeat_identical=same)
-        np.savez_compressed(os.path.join(HERE, "ref_grey32.npz"), Q=Q, sigma=S, meta=json.dumps(meta))
+        np.savez_compressed(os.path.join(a.outdir, "ref_grey32.npz"), Q=Q, sigma=S, meta=json.dumps(meta))
         print(json.dumps(meta))
         return
     runs, same = run_children("nb64", "nb64s0", a.repeats, tmp)
-    runs1, _ = run_children("nb64", "nb64", a.repeats, tmp)
-    Qf = runs[0]["Q"].astype(np.float64)
-    Sf = runs[0]["sigma"].astype(np.float64)
-    Q, S = Qf[1:-1, 1:-1, 1:-1], Sf[1:-1, 1:-1, 1:-1]
-    n = Q.shape[0] * Q.shape[1]
-    plane_mean = Q.mean(axis=(0, 1))
-    plane_se = np.sqrt((S ** 2).sum(axis=(0, 1))) / n
-    wq, ws = Qf[1:-1, 1:-1, 0], Sf[1:-1, 1:-1, 0]   # west-wall flux (i = 0)
+    runs1, same1 = run_children("nb64", "nb64", a.repeats, tmp)
+    runsf, samef = run_children("nb64", "nb64s0fix", a.repeats, tmp)
+
+    def split(run):
+        Qf = run["Q"].astype(np.float64)
+        Sf = run["sigma"].astype(np.float64)
+        Q, S = Qf[1:-1, 1:-1, 1:-1], Sf[1:-1, 1:-1, 1:-1]
+        n = Q.shape[0] * Q.shape[1]
+        # west-wall flux at i = 0 (get_results_ scatter, mc_gpu_noint.cu:996-1001)
+        return Q, S, Q.mean(axis=(0, 1)), np.sqrt((S ** 2).sum(axis=(0, 1))) / n, Qf[1:-1, 1:-1, 0], Sf[1:-1, 1:-1, 0]
+
+    Q, S, plane_mean, plane_se, wq, ws = split(runs[0])
+    _, _, plane_mean1, plane_se1, wq1, ws1 = split(runs1[0])
+    Qx, _, _, _, wqf, wsf = split(runsf[0])
+    for name, arr in (("srt0 Q", Q), ("srt0 wall", wq), ("srt1 plane", plane_mean1), ("srt1 wall", wq1),
+                      ("fixed-edge wall", wqf)):
+        assert np.all(np.isfinite(arr)), "reference returned non-finite %s" % name
     rng = np.random.default_rng(NB_SAMPLE_SEED)
     flat = rng.choice(Q.size, size=NB_SAMPLE, replace=False)
     idx = np.stack(np.unravel_index(flat, Q.shape), axis=1).astype(np.int16)
     meta = dict(config="nb64", field_seed=FIELD_SEED, srt=0, ms=[float(r["ms"]) for r in runs],
-                ms_srt1=[float(r["ms"]) for r in runs1], repeat_identical=same, sample_seed=NB_SAMPLE_SEED)
-    np.savez_compressed(os.path.join(HERE, "ref_nb64.npz"), plane_mean=plane_mean, plane_se=plane_se,
-                        wall_mean=wq.mean(), wall_se=np.sqrt((ws ** 2).sum()) / wq.size, sample_idx=idx,
-                        sample_Q=Q.reshape(-1)[flat], sample_sigma=S.reshape(-1)[flat], meta=json.dumps(meta))
+                ms_srt1=[float(r["ms"]) for r in runs1], repeat_identical=same, repeat_identical_srt1=same1,
+                repeat_identical_fix=samef, fix_fluid_identical=bool(np.array_equal(Qx, Q)),
+                sample_seed=NB_SAMPLE_SEED, walls="west (adiabatic), kernel_surface emission patched")
+    np.savez_compressed(os.path.join(a.outdir, "ref_nb64.npz"), plane_mean=plane_mean, plane_se=plane_se,
+                        wall_q=wq.astype(np.float32), wall_sigma=ws.astype(np.float32),
+                        sample_idx=idx, sample_Q=Q.reshape(-1)[flat], sample_sigma=S.reshape(-1)[flat],
+                        srt1_plane_mean=plane_mean1, srt1_plane_se=plane_se1,
+                        srt1_wall_q=wq1.astype(np.float32), srt1_wall_sigma=ws1.astype(np.float32),
+                        fix_wall_q=wqf.astype(np.float32), fix_wall_sigma=wsf.astype(np.float32),
+                        meta=json.dumps(meta))
     print(json.dumps(meta))
 
 

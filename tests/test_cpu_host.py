@@ -5,12 +5,15 @@ import os
 import numpy as np
 import pytest
 
+from oracle.ref_build import REF
 from radchan_b200 import api
 from radchan_b200 import workloads as W
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 GOLD = os.path.join(HERE, "golden")
-REF_PARAM = "/root/reference/src/param"
+# the reference checkout's parameter headers, where the reference build
+# recipe finds the checkout (skipped when it is absent)
+REF_PARAM = os.path.join(REF, "src", "param")
 
 
 def test_parse_channel_headers():

@@ -2,9 +2,9 @@
 table, field and partial-sum index of the march is checked against its
 array on the device.  Small cases covering each path (grey, narrow band
 with levels, every wall type, both wall fluxes, a z slab, band-sorted
-order, the FP64 build, a batch, the server) run in a child process that
-loads the checked library; none may flag an index (status bit 3) and each
-result must equal the oracle bit for bit."""
+order, the FP64 build, a batch, the server, the allocation-free solve) run
+in a child process that loads the checked library; none may flag an index
+(status bit 3) and each result must equal the oracle bit for bit."""
 import json
 import os
 import subprocess
@@ -77,6 +77,24 @@ def child():
     r = srv.wait(srv.submit(p, T, table_set=srv.add_tables(tabs)))
     srv.close()
     res["server"] = dict(status=0, equal=bool(np.array_equal(r.Q, alone.Q)))
+    # the allocation-free entry point reports status bit 3 through its return
+    # code (RC_E_RANGE) and message
+    import ctypes as C
+    import torch
+    s = api.Solver(p, tabs)
+    dp = lambda t: C.c_void_p(t.data_ptr())
+    kl = p.kmax // p.p_col
+    q = torch.full((kl, p.jmax, p.imax), float("nan"), dtype=torch.float64, device="cuda")
+    v, qw = torch.full_like(q, float("nan")), torch.full((2, kl, p.jmax), float("nan"), dtype=torch.float64,
+                                                         device="cuda")
+    vw = torch.full_like(qw, float("nan"))
+    rc = L.lib().rc_solve_noalloc(s.ctx, dp(torch.from_numpy(T).cuda()), 1, dp(q), dp(v), dp(qw), dp(vw))
+    msg = L.last_error(s.ctx) if rc else ""
+    o = O.solve(p, tabs, T, rpt=s.get_launch()[0])
+    res["noalloc"] = dict(status=8 if "out of bounds" in msg else (0 if rc == 0 else -1), rc=rc, msg=msg,
+                          equal=bool(np.array_equal(q.cpu().numpy(), o["q64"]) and
+                                     np.array_equal(qw.cpu().numpy(), o["qw64"])))
+    s.close()
     print(json.dumps(res))
 
 
@@ -89,8 +107,9 @@ def test_checked_build_flags_nothing_and_matches_the_oracle():
                        capture_output=True, text=True, timeout=900)
     assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-4000:]
     res = json.loads(r.stdout.strip().splitlines()[-1])
-    assert len(res) == 9
+    assert len(res) == 10
     for name, v in res.items():
+        assert v["status"] >= 0, (name, v)
         assert v["status"] & 8 == 0, (name, v["status"] >> 8)
         assert v["equal"], name
 

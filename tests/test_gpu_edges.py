@@ -79,3 +79,38 @@ def test_bad_arguments_fail_before_launch():
     with pytest.raises(L.RadChanError):
         api.Solver(q)
     s.close()
+
+
+@pytest.mark.parametrize("grey", [False, True])
+def test_band_and_g_search_edges_equal_the_oracle(grey):
+    """The device's band / g-point searches (select_band_g, used by every
+    emission) against the oracle on uniforms placed on, just below and just
+    above every CDF entry, at 0, just below 1 and at 1; the oracle follows
+    the reference's bisection rule on the same uniforms
+    (tests/test_cpu_band_search.py)."""
+    from test_cpu_band_search import _problem, edge_uniforms
+    O = _oracle()
+    p, tabs, T = _problem(grey)
+    s = api.Solver(p, tabs)
+    t = s.solve_async(T)
+    _, _, cdf_f, cdf_s, probq, row = O.sample_bands(p, tabs, T, 0, [0.5], [0.5])
+    cases = [(0, edge_uniforms(cdf_f), None)]
+    cases.append((1, np.unique(np.concatenate([edge_uniforms(cdf_s), edge_uniforms(cdf_f[:1], n_random=0)])), None))
+    if not grey:
+        a = tabs.arrays()
+        for b in (0, 7, 39):
+            ub = np.float32(np.nextafter(cdf_f[b], np.float32(0)))
+            ug = edge_uniforms(a["probg"][row, b], seed=b, n_random=50)
+            cases.append((0, np.full_like(ug, ub), ug))
+        cases.append((2, np.full(60, 0.5, np.float32), edge_uniforms(probq, n_random=50)[:60]))
+    for kind, ub, ug in cases:
+        if ug is None:
+            ug = np.full_like(ub, 0.5)
+        n = min(ub.size, ug.size)
+        ub, ug = ub[:n], ug[:n]
+        nb_d, g_d = s.sample_bands(t, kind, ub, ug)
+        nb_o, g_o, _, _, _, _ = O.sample_bands(p, tabs, T, kind, ub, ug)
+        assert np.array_equal(nb_d, nb_o), kind
+        assert np.array_equal(g_d, g_o), kind
+    s.release(t)
+    s.close()

@@ -1,17 +1,36 @@
-"""Statistical parity with the reference's own CUDA solver.
+"""Statistical parity with the reference's own CUDA solver, run on the B200.
 
-tests/golden/ref_grey32.npz holds Q and sigma of every cell of the grey
-32^3 channel (kappa = 1/m, black walls 955 K / 573 K, periodic y/z,
-photmax 64, nVar 4) computed by RadChan's mc_gpu_/get_results_ built for
-the B200 (oracle/ref_build.py, generated by tests/golden/make_ref_fixtures.py).
-tests/golden/ref_nb64.npz holds the same solver's narrow-band 64^3 channel
-(100 bands x 8 g points of the seeded synthetic tables, 3 levels, photmax
-256, nVar 4, built with srt = 0): per-x-plane means of Q with their standard
-errors and Q, sigma of 4096 sampled cells.  (Its west-wall fluxes came back
-NaN from the reference, so walls are not compared.)
-The reference's generators (cuRAND XORWOW) differ from ours (Philox), so
-agreement is statistical: per-x-plane means of Q must agree within 4.5
-combined standard errors, and the per-cell z-scores must centre on 0.
+Fixtures (tests/golden/make_ref_fixtures.py, built by oracle/ref_build.py):
+  ref_grey32.npz  Q and sigma of every cell of the grey 32^3 channel
+                  (kappa = 1/m, black walls 955 K / 573 K, periodic y/z,
+                  photmax 64, nVar 4);
+  ref_nb64.npz    the narrow-band 64^3 channel of the benchmark (100 bands x
+                  8 g, 3 levels, photmax 256, nVar 4, adiabatic west wall):
+                  srt 0 build: x-plane means of Q and their standard errors,
+                  Q and sigma of 4096 sampled cells, west-wall flux and sigma
+                  of every wall cell; srt 1 build (as configured): x-plane
+                  means, west-wall flux; srt 0 build with find_bandS's edge
+                  rule corrected: west-wall flux.
+
+The reference draws cuRAND XORWOW, this solver Philox, so agreement is
+statistical; the criteria (tests/mc_stats.py) are the north star's "within 3
+combined standard deviations from nVar independent runs": per cell, the
+count of |z| > 3 against its null distribution for 4-replicate sigmas; for
+aggregates (x planes, the wall mean), |z| < 3 at a family-wise error of
+0.27%.
+
+Two documented divergences shape the wall comparison:
+  * find_bandS tests the wall draw against the fluid CDF's first entry
+    (mc_gpu_noint.cu:1189,1208).  This solver uses the wall CDF's own.  The
+    oracle can apply either rule (oracle_set_ref_wall_edge) with the same
+    draws; with the reference's rule it reproduces the reference's west-wall
+    flux, with the corrected rule it matches the reference build whose edge
+    rule is corrected, and both solvers shift by the same amount between
+    the rules.
+  * srt 1 replays one band histogram per thread for all nVar replicates
+    (mc_gpu_noint.cu:89-110), so its reported sigma understates its error.
+    Its x-plane means are compared with a standard error bounded by twice
+    the srt 0 build's (the replicates at most fully correlated).
 """
 import json
 import os
@@ -19,10 +38,12 @@ import os
 import numpy as np
 import pytest
 
+import mc_stats as MS
 from radchan_b200 import workloads as W
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 FIX = os.path.join(HERE, "golden", "ref_grey32.npz")
+NB_FIX = os.path.join(HERE, "golden", "ref_nb64.npz")
 
 
 def _fixture():
@@ -30,24 +51,62 @@ def _fixture():
     return d["Q"].astype(np.float64), d["sigma"].astype(np.float64), json.loads(str(d["meta"]))
 
 
+def _nb():
+    return np.load(NB_FIX)
+
+
 def check_against_reference(Q, S):
+    """grey 32^3: every x plane and every cell."""
     Qr, Sr, _ = _fixture()
     assert Q.shape == Qr.shape
-    n = Qr.shape[0] * Qr.shape[1]
-    se = np.sqrt((Sr ** 2).sum(axis=(0, 1)) + (S ** 2).sum(axis=(0, 1))) / n
-    zp = (Q.mean(axis=(0, 1)) - Qr.mean(axis=(0, 1))) / se
-    assert np.all(np.abs(zp) < 4.5), zp
-    z = (Q - Qr) / np.sqrt(S ** 2 + Sr ** 2)
-    assert abs(z.mean()) < 0.05
-    assert 0.7 < z.std() < 1.6
+    pa = MS.aggregates(*MS.plane_stats(Q, S), *MS.plane_stats(Qr, Sr))
+    assert pa["ok"], pa
+    pc = MS.per_cell(Q, S, Qr, Sr)
+    assert pc["ok"], pc
     # the x-profile of the source has the reference's shape
-    pr = Qr.mean(axis=(0, 1))
-    assert np.corrcoef(pr, Q.mean(axis=(0, 1)))[0, 1] > 0.999
+    assert np.corrcoef(Qr.mean(axis=(0, 1)), Q.mean(axis=(0, 1)))[0, 1] > 0.999
 
 
+def check_against_reference_nb64(Q, S):
+    """narrow-band 64^3 fluid cells: x planes of the srt 0 build, the 4096
+    sampled cells, and x planes of the srt 1 build."""
+    d = _nb()
+    pm, pse = MS.plane_stats(Q, S)
+    pa = MS.aggregates(pm, pse, d["plane_mean"], d["plane_se"])
+    assert pa["ok"], pa
+    idx = d["sample_idx"].astype(int)
+    qs, ss = Q[idx[:, 0], idx[:, 1], idx[:, 2]], S[idx[:, 0], idx[:, 1], idx[:, 2]]
+    pc = MS.per_cell(qs, ss, d["sample_Q"], d["sample_sigma"])
+    assert pc["ok"], pc
+    assert np.corrcoef(pm, d["plane_mean"])[0, 1] > 0.999
+    # srt 1: standard error bounded by twice the srt 0 build's
+    p1 = MS.aggregates(pm, pse, d["srt1_plane_mean"], 2.0 * d["plane_se"])
+    assert p1["ok"], p1
+
+
+def check_walls(qw, vw, which):
+    """West-wall flux [k, j] against a reference build: its mean over the
+    wall and every wall cell."""
+    d = _nb()
+    wq, ws = d[which + "_q"].astype(np.float64), d[which + "_sigma"].astype(np.float64)
+    s = np.sqrt(vw)
+    wa = MS.aggregates(*MS.wall_stats(qw, s), *MS.wall_stats(wq, ws))
+    assert wa["ok"], (which, wa)
+    pc = MS.per_cell(qw, s, wq, ws)
+    assert pc["ok"], (which, pc)
+    return wa
+
+
+# ------------------------------------------------------------------ grey
 def test_fixture_metadata():
     _, _, meta = _fixture()
     assert meta["config"] == "grey32" and meta["repeat_identical"]
+
+
+def test_null_model_of_the_per_cell_criterion():
+    # two 4-replicate solves of one estimator: |z| > 3 in 1.85% of cells
+    assert abs(MS.exceed_prob(4, 4) - 0.0185) < 0.0005
+    assert abs(MS.family_threshold(64) - 4.095) < 0.01
 
 
 def test_oracle_matches_reference_cuda_build():
@@ -57,6 +116,19 @@ def test_oracle_matches_reference_cuda_build():
     T = W.channel_field(p, seed=meta["field_seed"])
     o = O.solve(p, None, T, rpt=4)
     check_against_reference(o["q64"], np.sqrt(o["var64"]))
+
+
+def test_a_planted_bias_fails_the_criterion():
+    """The criterion has power: the oracle's own solve with its source
+    raised by 3% of the mean |Q| in one x plane (planted on the CPU) fails."""
+    from oracle import oracle as O
+    _, _, meta = _fixture()
+    p = W.config_grey_32()
+    o = O.solve(p, None, W.channel_field(p, seed=meta["field_seed"]), rpt=4)
+    Q = o["q64"].copy()
+    Q[:, :, 16] += 0.03 * np.abs(Q).mean()
+    with pytest.raises(AssertionError):
+        check_against_reference(Q, np.sqrt(o["var64"]))
 
 
 @pytest.mark.gpu
@@ -70,42 +142,77 @@ def test_gpu_matches_reference_cuda_build(photmax):
     check_against_reference(r.q64, np.sqrt(r.var64))
 
 
-NB_FIX = os.path.join(HERE, "golden", "ref_nb64.npz")
-
-
-def check_against_reference_nb64(Q, S):
-    d = np.load(NB_FIX)
-    n = Q.shape[0] * Q.shape[1]
-    pm = Q.mean(axis=(0, 1))
-    pse = np.sqrt((S ** 2).sum(axis=(0, 1))) / n
-    zp = (pm - d["plane_mean"]) / np.sqrt(pse ** 2 + d["plane_se"] ** 2)
-    assert np.all(np.abs(zp) < 4.5), zp
-    assert abs(zp.mean()) < 0.5
-    idx = d["sample_idx"].astype(int)
-    qs, ss = Q[idx[:, 0], idx[:, 1], idx[:, 2]], S[idx[:, 0], idx[:, 1], idx[:, 2]]
-    z = (qs - d["sample_Q"]) / np.sqrt(ss ** 2 + d["sample_sigma"] ** 2)
-    assert abs(z.mean()) < 0.1
-    assert 0.7 < z.std() < 1.6
-    assert np.corrcoef(pm, d["plane_mean"])[0, 1] > 0.999
-
-
+# ---------------------------------------------------------- narrow band
 def test_nb64_fixture_metadata():
-    meta = json.loads(str(np.load(NB_FIX)["meta"]))
+    meta = json.loads(str(_nb()["meta"]))
     assert meta["config"] == "nb64" and meta["srt"] == 0 and meta["field_seed"] == 7
+    assert meta["repeat_identical"] and meta["repeat_identical_srt1"] and meta["repeat_identical_fix"]
+    # the edge-rule patch touches only the wall kernel
+    assert meta["fix_fluid_identical"]
+    d = _nb()
+    for k in ("wall_q", "srt1_wall_q", "fix_wall_q", "srt1_plane_mean"):
+        assert np.all(np.isfinite(d[k])), k
 
 
 def test_oracle_matches_reference_cuda_build_narrowband():
     from oracle import oracle as O
     p = W.config_nb_64()
-    T = W.channel_field(p, seed=json.loads(str(np.load(NB_FIX)["meta"]))["field_seed"])
+    T = W.channel_field(p, seed=json.loads(str(_nb()["meta"]))["field_seed"])
     o = O.solve(p, W.tables_nb(), T, rpt=4)
     check_against_reference_nb64(o["q64"], np.sqrt(o["var64"]))
+    check_walls(o["qw64"][0], o["vw64"][0], "fix_wall")
+
+
+def _oracle_walls(rule, rpt=4, p=None):
+    from oracle import oracle as O
+    p = p or W.config_nb_64()
+    T = W.channel_field(p, seed=json.loads(str(_nb()["meta"]))["field_seed"])
+    O.lib().oracle_set_ref_wall_edge(rule)
+    try:
+        return O.solve(p, W.tables_nb(), T, rpt=rpt, cell_begin=0, cell_end=0, walls=True)
+    finally:
+        O.lib().oracle_set_ref_wall_edge(0)
+
+
+def test_oracle_with_the_reference_edge_rule_reproduces_the_reference_walls():
+    o = _oracle_walls(1)
+    check_walls(o["qw64"][0], o["vw64"][0], "wall")
+    # srt 1 (the same defect through kernel_findS): the wall mean only, with
+    # its standard error bounded by twice the srt 0 build's; its per-cell
+    # sigmas come from replicates sharing one band histogram and are far too
+    # small for a per-cell test
+    d = _nb()
+    m1 = d["srt1_wall_q"].astype(np.float64).mean()
+    _, se0 = MS.wall_stats(d["wall_q"], d["wall_sigma"])
+    wa = MS.aggregates(*MS.wall_stats(o["qw64"][0], np.sqrt(o["vw64"][0])), m1, 2.0 * se0)
+    assert wa["ok"], wa
+
+
+def test_the_edge_rule_defect_shifts_both_solvers_alike():
+    """Same draws, two rules: the shift of the wall mean is the defect's
+    effect.  The oracle's shift (Philox draws) and the reference's shift
+    between its unpatched and corrected builds (XORWOW draws) agree within
+    3 combined standard errors of the paired differences."""
+    a, b = _oracle_walls(1)["qw64"][0], _oracle_walls(0)["qw64"][0]
+    d = _nb()
+    r = d["wall_q"].astype(np.float64) - d["fix_wall_q"].astype(np.float64)
+    do = a - b
+    z = (do.mean() - r.mean()) / np.sqrt(do.var() / do.size + r.var() / r.size)
+    assert do.mean() > 0 and r.mean() > 0
+    assert abs(z) < 3, (do.mean(), r.mean(), z)
 
 
 @pytest.mark.gpu
 def test_gpu_matches_reference_cuda_build_narrowband():
     from radchan_b200 import api
     p = W.config_nb_64()
-    T = W.channel_field(p, seed=json.loads(str(np.load(NB_FIX)["meta"]))["field_seed"])
-    r = api.Solver(p, W.tables_nb()).solve(T)
+    T = W.channel_field(p, seed=json.loads(str(_nb()["meta"]))["field_seed"])
+    s = api.Solver(p, W.tables_nb())
+    r = s.solve(T)
     check_against_reference_nb64(r.q64, np.sqrt(r.var64))
+    # walls: the device's west-wall fluxes equal the oracle's bit for bit
+    # (same draws, corrected edge rule) and agree with the reference build
+    # whose edge rule is corrected
+    o = _oracle_walls(0, rpt=s.get_launch()[0])
+    assert np.array_equal(r.qw64[0], o["qw64"][0]) and np.array_equal(r.vw64[0], o["vw64"][0])
+    check_walls(r.qw64[0], r.vw64[0], "fix_wall")
