@@ -314,6 +314,24 @@ def run_reference(args, ws, rank):
     print(json.dumps(line), flush=True)
 
 
+def gather_ceilings(p, achieved_gbs, dev):
+    """The march's gathers stay in L2 (the temperature pyramid of every level
+    as uint16 coordinates plus the interleaved k / I_b table rows), so next
+    to the HBM convention its achieved 32 B/step rate is stated against the
+    random-sector gather throughput this GPU delivers over an array of that
+    size (rc_probe_gather): L2 only, and through L1 as the march reads."""
+    from radchan_b200 import api
+    cells = sum(p.maxi[l] * p.maxj[l] * p.maxk[l] for l in range(p.grid_num))
+    nB, nQ, nT = (p.grey_nB, 1, p.grey_nT) if p.grey else (p.nB, p.nQ, p.nT)
+    ws = 2 * cells + 16 * nB * nQ * nT
+    _, l2, _ = api.probe_gather(ws, mode=0, device=dev)
+    _, l1l2, _ = api.probe_gather(ws, mode=1, device=dev)
+    return {"working_set_bytes": ws, "l2_gather_gbs": l2, "frac_l2": achieved_gbs / l2,
+            "l1l2_gather_gbs": l1l2, "frac_l1l2": achieved_gbs / l1l2,
+            "gather_probe": "rc_probe_gather: 4 B from a random 32 B sector per lane, 8 in flight, full occupancy; "
+                            "GB/s = sectors/s x 32"}
+
+
 def leg_at_tolerance(p, tabs, T, rel0, dev, flush, tol=0.01, steps=2):
     """The same solve with photmax raised until the relative standard
     deviation of max|Q| is `tol` (it falls as photmax^-1/2): device time per
@@ -464,6 +482,13 @@ def leg_batched(dev, passes=2, **mix):
             it["s"].collect_into(it["s"].solve_async(it["T"]), it["Q"], it["S"])
         return time.perf_counter() - t0
 
+    # ray-cell steps of one pass (the mix's problems take very different
+    # numbers of steps per bundle, so steps/s is the comparable rate)
+    steps = 0.0
+    for it in items:
+        t = it["s"].solve_async(it["T"])
+        steps += it["s"].info(t).steps
+        it["s"].release(t)
     plain_pass()
     t_plain = min(plain_pass() for _ in range(passes))
     ref = [it["Q"].copy() for it in items]
@@ -507,6 +532,8 @@ def leg_batched(dev, passes=2, **mix):
             "plain_solves_per_s": n / t_plain, "batched_solves_per_s": n / t_batch, "served_solves_per_s": n / t_srv,
             "batched_vs_plain": t_plain / t_batch, "served_vs_plain": t_plain / t_srv,
             "plain_bundles_per_s": bundles / t_plain, "batched_bundles_per_s": bundles / t_batch,
+            "steps_per_pass": steps, "steps_per_bundle": steps / bundles,
+            "plain_steps_per_s": steps / t_plain, "batched_steps_per_s": steps / t_batch,
             "batched_equals_plain": identical, "timing": "wall clock per pass of all solves, host arrays in/out, "
                                                         "best of %d" % passes}
 
@@ -728,6 +755,7 @@ def run_ours(args, ws, rank, local):
     roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
             "traffic": traffic, "kernel": "k_march", "peak_source": peak_kind,
             "algorithmic_bytes_per_step": 32, "steps_per_launch": steps / args.steps}
+    roof.update(gather_ceilings(p, achieved, dev))
     line = {"metric": BUNDLE_METRIC, "value": value, "unit": "bundles/s", "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": 1000 * t_max / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",

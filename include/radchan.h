@@ -302,6 +302,19 @@ int rc_trace(rc_ctx *ctx, rc_ticket ticket, int n, const rc_bundle_id *ids,
 int rc_sample_bands(rc_ctx *ctx, rc_ticket ticket, int kind, int n, const float *u_band,
                     const float *u_g, int *nb, int *g);
 
+/* ---------------- diagnostics ---------------- */
+
+/* Random-sector gather throughput of this GPU (no counterpart in the
+ * reference): every lane reads 4 bytes from a pseudo-random 32-byte sector
+ * of a device array of `bytes` bytes, eight independent reads in flight,
+ * at full occupancy; mode 0 reads through L2 only (ld.global.cg), mode 1
+ * through the read-only L1 path as the march does.  *sectors_per_s is the
+ * best of three timed launches after a warm-up launch (CUDA events);
+ * *ms_best (optional) that launch's time.  With `bytes` at the size of a
+ * solve's temperature pyramid and tables it is the ceiling of the march's
+ * gathers, which stay L2-resident. */
+int rc_probe_gather(int device, size_t bytes, int mode, int iters, double *sectors_per_s, float *ms_best);
+
 /* ---------------- batched solves ---------------- */
 
 typedef struct rc_batch rc_batch;

@@ -133,6 +133,7 @@ _SIGS = [
     ("rc_debug_fail_next", _I, [C.c_char_p, _I]),
     ("rc_grid_level", _I, [C.POINTER(RcParams), _I, _FP, _FP, _FP, _FP, _FP, _FP]),
     ("rc_trace", _I, [_VP, C.c_int32, _I, C.POINTER(RcBundleId), C.POINTER(RcTraceRec), _I, C.POINTER(C.c_int)]),
+    ("rc_probe_gather", _I, [_I, C.c_size_t, _I, _I, C.POINTER(C.c_double), C.POINTER(C.c_float)]),
     ("rc_sample_bands", _I, [_VP, C.c_int32, _I, _I, _FP, _FP, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
     ("rc_batch_create", _I, [_I, _I, C.POINTER(_VP)]),
     ("rc_batch_add", _I, [_VP, _VP, _FP, _I]),

@@ -142,6 +142,16 @@ def compare_in_sigma(a: "Result", b: "Result"):
     return out
 
 
+def probe_gather(nbytes: int, mode: int = 0, iters: int = 1024, device: int = 0):
+    """rc_probe_gather: random 32-byte-sector gather throughput over an
+    array of nbytes (mode 0 L2 only, mode 1 through L1); returns (sectors/s,
+    GB/s at 32 B per sector, ms of the best launch)."""
+    s = C.c_double()
+    ms = C.c_float()
+    L.check(L.lib().rc_probe_gather(device, int(nbytes), mode, iters, C.byref(s), C.byref(ms)))
+    return s.value, s.value * 32 / 1e9, ms.value
+
+
 def field_shape(p):
     """numpy shape of the temperature field: (kmax+2, jmax+2, imax+2), i fastest."""
     return (p.kmax + 2, p.jmax + 2, p.imax + 2)
