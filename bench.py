@@ -462,35 +462,60 @@ def batch_setup(dev, n=64, edges=(16, 24, 32, 48, 64, 96), photmaxes=(32, 128, 5
     return items
 
 
-def leg_batched(dev, passes=2, **mix):
+def leg_batched(dev, passes=2, tol=None, max_bundles=2.5e11, served=True, warm=True, **mix):
     """Plain (one solve per launch, host arrays in and out, one after the
     other) vs batched (every solve in one persistent launch replayed from a
     CUDA graph) vs served (all submitted to the continuous-batching server at
-    once) on the uneven mix.  Wall clock per pass of all 64 solves."""
+    once) on the uneven mix.  Wall clock per pass of all 64 solves.  With
+    `tol`, every problem first runs a pilot at its recipe photmax and then
+    uses the photmax that brings the relative standard deviation of its
+    max|Q| to tol (it falls as photmax^-1/2): the comparison at equal
+    tolerance.  warm=False skips the untimed first pass of each mode (the
+    pilots have run every problem once; the batch's graph is captured inside
+    its timed pass, which costs well under 1% of a pass at this size)."""
+    import math
+
     from radchan_b200 import api
     items = batch_setup(dev, **mix)
+    if tol is not None:
+        for it in items:
+            r = it["s"].solve(it["T"])
+            rel = api.rel_std_maxq(r.q64, np.sqrt(r.var64))
+            q = api.copy_params(it["p"])
+            q.photmax = int(math.ceil(it["p"].photmax * (rel / tol) ** 2))
+            it["s"].close()
+            it["p"] = q
+            it["s"] = api.Solver(q, it["tabs"], device=dev)
     work = [it["p"].imax * it["p"].jmax * it["p"].kmax * it["p"].nVar * it["p"].photmax for it in items]
+    if sum(work) > max_bundles:
+        for it in items:
+            it["s"].close()
+        return {"skipped": "%.3g bundles per pass exceed the leg's bound %.3g" % (sum(work), max_bundles)}
     big = items[int(np.argmax(work))]
     knobs = big["s"].autotune(big["T"], pilot_photmax=min(big["p"].photmax, 128))
     for it in items:
         it["s"].set_launch(*knobs)
     bundles = float(sum(work))
 
+    # ray-cell steps of one pass, read from each solve's info (the mix's
+    # problems take very different numbers of steps per bundle, so steps/s
+    # is the comparable rate)
+    steps_seen = []
+
     def plain_pass():
         t0 = time.perf_counter()
+        n = 0.0
         for it in items:
-            it["s"].collect_into(it["s"].solve_async(it["T"]), it["Q"], it["S"])
+            t = it["s"].solve_async(it["T"])
+            n += it["s"].info(t).steps
+            it["s"].collect_into(t, it["Q"], it["S"])
+        steps_seen.append(n)
         return time.perf_counter() - t0
 
-    # ray-cell steps of one pass (the mix's problems take very different
-    # numbers of steps per bundle, so steps/s is the comparable rate)
-    steps = 0.0
-    for it in items:
-        t = it["s"].solve_async(it["T"])
-        steps += it["s"].info(t).steps
-        it["s"].release(t)
-    plain_pass()
+    if warm:
+        plain_pass()
     t_plain = min(plain_pass() for _ in range(passes))
+    steps = steps_seen[-1]
     ref = [it["Q"].copy() for it in items]
     b = api.Batch(device=dev, use_graph=True)
     for it in items:
@@ -504,10 +529,24 @@ def leg_batched(dev, passes=2, **mix):
             b.collect_into(i, it["Q"], it["S"])
         return time.perf_counter() - t0
 
-    batched_pass()
+    if warm:
+        batched_pass()
     t_batch = min(batched_pass() for _ in range(passes))
     identical = all(np.array_equal(r, it["Q"]) for r, it in zip(ref, items))
     b.close()
+    if not served:
+        for it in items:
+            it["s"].close()
+        n = len(items)
+        return {"problems": n, "bundles_per_pass": bundles, "tolerance": tol,
+                "photmax_range": [min(it["p"].photmax for it in items), max(it["p"].photmax for it in items)],
+                "plain_solves_per_s": n / t_plain, "batched_solves_per_s": n / t_batch,
+                "batched_vs_plain": t_plain / t_batch, "plain_bundles_per_s": bundles / t_plain,
+                "batched_bundles_per_s": bundles / t_batch, "steps_per_pass": steps,
+                "plain_steps_per_s": steps / t_plain, "batched_steps_per_s": steps / t_batch,
+                "batched_equals_plain": identical,
+                "timing": "wall clock per pass of all solves, host arrays in/out, best of %d after one warm-up "
+                          "pass" % passes}
     srv = api.Server(device=dev, max_inflight=len(items))
 
     def served_pass():
@@ -526,7 +565,8 @@ def leg_batched(dev, passes=2, **mix):
     for it in items:
         it["s"].close()
     n = len(items)
-    return {"problems": n, "bundles_per_pass": bundles,
+    return {"problems": n, "bundles_per_pass": bundles, "tolerance": tol,
+            "photmax_range": [min(it["p"].photmax for it in items), max(it["p"].photmax for it in items)],
             "autotuned": {"rays_per_thread": knobs[0], "block_threads": knobs[1], "sort_bands": knobs[2],
                           "occupancy": knobs[3]},
             "plain_solves_per_s": n / t_plain, "batched_solves_per_s": n / t_batch, "served_solves_per_s": n / t_srv,
@@ -538,21 +578,22 @@ def leg_batched(dev, passes=2, **mix):
                                                         "best of %d" % passes}
 
 
-def run_serve(args, rank, local):
+def serve_run(dev, n_requests, load, inflight=32, policy="srpt", wall_cap=None, seed=2024):
     """Open-loop serving: Poisson arrivals of narrow-band solve requests
-    (100 bands x 8 g) with grids drawn log-uniformly from 32^3 to
-    256x128x128 (eight size classes), tolerance drawn log-uniformly from
-    1% to 5% relative std of max|Q| (photmax chosen by the server), fields
-    and tables resident, admission by a 150 GB budget.  The arrival rate is
-    args.load x the capacity 1 / E[service time alone] of the mix, with the
-    service time of every size class measured alone after calibration."""
-    if rank != 0:
-        return
+    (100 bands x 8 g) with grids drawn from eight classes log-spaced from
+    32^3 to 256x128x128, tolerance drawn log-uniformly from 1% to 5%
+    relative std of max|Q| (photmax chosen by the server), fields and tables
+    resident, admission by a 150 GB budget.  The arrival rate is `load` x
+    the capacity 1 / E[service time alone] of the mix, with the service
+    time of every size class measured alone after calibration.  With
+    wall_cap (seconds) no request is submitted after that time; the ones
+    submitted all complete and are reported."""
+    import queue
     import threading
 
     from radchan_b200 import api
     from radchan_b200 import workloads as W
-    rng = np.random.default_rng(2024)
+    rng = np.random.default_rng(seed)
     tabs = W.tables_nb()
     classes = []
     for c in range(8):
@@ -563,18 +604,12 @@ def run_serve(args, rank, local):
                                                                      (im // 4, jm // 4, jm // 4)],
                              maxs=[5, 5, 100000], calcwalls=1, adiabw=1)
         classes.append((p, W.channel_field(p, seed=100 + c)))
-    srv = api.Server(device=local, hbm_budget_bytes=150e9, max_inflight=args.serve_inflight)
-    srv.set_policy(args.policy)
+    srv = api.Server(device=dev, hbm_budget_bytes=150e9, max_inflight=inflight)
+    srv.set_policy(policy)
     ts = srv.add_tables(tabs)
-
-    def draw(n):
-        out = []
-        for _ in range(n):
-            c = int(rng.integers(0, 8))
-            tol = float(np.exp(rng.uniform(np.log(0.01), np.log(0.05))))
-            out.append((c, tol))
-        return out
-
+    reqs = []
+    for _ in range(n_requests):
+        reqs.append((int(rng.integers(0, 8)), float(np.exp(rng.uniform(np.log(0.01), np.log(0.05))))))
     # calibration of every class (pilot + one solve at 3%), then the service
     # time of each class alone at its calibrated photmax (no other request)
     alone = []
@@ -583,59 +618,81 @@ def run_serve(args, rank, local):
         r = srv.wait(srv.submit(p, T, table_set=ts, tolerance=0.03))
         alone.append((r.t_done - r.t_admit, r.photmax))
     # capacity: one over the mean service time alone of the request mix
-    # (photmax grows as 1/tol^2 from the 3% calibration); concurrent small
-    # requests share the GPU better than that, so the load is conservative
-    reqs = draw(args.serve_requests)
+    # (photmax grows as 1/tol^2 from the 3% calibration)
     mean_svc = float(np.mean([alone[c][0] * (0.03 / tol) ** 2 for c, tol in reqs]))
     cap = 1.0 / mean_svc
-    rate = args.load * cap
+    rate = load * cap
     gaps = rng.exponential(1.0 / rate, size=len(reqs))
-    results = [None] * len(reqs)
-    ids = [None] * len(reqs)
-    ready = threading.Semaphore(0)
+    results = []
+    pending = queue.Queue()
 
     def waiter():
-        for i in range(len(reqs)):
-            ready.acquire()
-            results[i] = srv.wait(ids[i])
+        while True:
+            item = pending.get()
+            if item is None:
+                return
+            i, rid = item
+            results.append((i, srv.wait(rid)))
 
     th = threading.Thread(target=waiter)
     th.start()
     st0 = srv.stats()
     t0 = time.perf_counter()
     t_next = t0
+    n_sub = 0
     for i, (c, tol) in enumerate(reqs):
         t_next += gaps[i]
+        if wall_cap is not None and t_next - t0 > wall_cap:
+            break
         d = t_next - time.perf_counter()
         if d > 0:
             time.sleep(d)
-        ids[i] = srv.submit(classes[c][0], classes[c][1], table_set=ts, tolerance=tol)
-        ready.release()
+        pending.put((i, srv.submit(classes[c][0], classes[c][1], table_set=ts, tolerance=tol)))
+        n_sub += 1
+    pending.put(None)
     th.join()
     wall = time.perf_counter() - t0
     st1 = srv.stats()
     srv.close()
-    lat = np.array([r.latency for r in results])
+    results.sort(key=lambda x: x[0])
+    done = [reqs[i] for i, _ in results]
+    res = [r for _, r in results]
+    lat = np.array([r.latency for r in res])
     # service time alone, scaled by photmax from the class's calibration solve
-    svc = np.array([alone[c][0] * r.photmax / alone[c][1] for r, (c, _) in zip(results, reqs)])
+    svc = np.array([alone[c][0] * r.photmax / alone[c][1] for r, (c, _) in zip(res, done)])
     slow = lat / svc
-    met = np.array([r.rel_std_maxq <= 1.25 * tol for r, (_, tol) in zip(results, reqs)])
-    line = {"metric": "serve latency p50/p99 and solves/s", "impl": "ours", "n_gpus": 1,
-            "requests": len(reqs), "load": args.load, "capacity_solves_per_s": cap, "policy": args.policy,
-            "offered_solves_per_s": rate, "solves_per_s": len(reqs) / wall,
-            "p50_s": float(np.percentile(lat, 50)), "p99_s": float(np.percentile(lat, 99)),
-            "p99_over_p50": float(np.percentile(lat, 99) / np.percentile(lat, 50)),
-            "alone_p50_s": float(np.percentile(svc, 50)), "alone_p99_s": float(np.percentile(svc, 99)),
-            "alone_p99_over_p50": float(np.percentile(svc, 99) / np.percentile(svc, 50)),
-            "slowdown_p50": float(np.percentile(slow, 50)), "slowdown_p99": float(np.percentile(slow, 99)),
-            "mean_photmax": float(np.mean([r.photmax for r in results])),
-            "tolerance_met_frac": float(met.mean()),
+    met = np.array([r.rel_std_maxq <= 1.25 * tol for r, (_, tol) in zip(res, done)])
+    pct = lambda a, q: float(np.percentile(a, q)) if len(a) else None
+    per_class = {}
+    for c, (p, _) in enumerate(classes):
+        m = np.array([cc == c for cc, _ in done], bool)
+        if m.any():
+            per_class["%dx%dx%d" % (p.imax, p.jmax, p.kmax)] = {
+                "requests": int(m.sum()), "p50_s": pct(lat[m], 50), "p99_s": pct(lat[m], 99),
+                "p99_over_p50": pct(lat[m], 99) / pct(lat[m], 50), "slowdown_p50": pct(slow[m], 50),
+                "slowdown_p99": pct(slow[m], 99), "alone_p50_s": pct(svc[m], 50)}
+    return {"requests": len(res), "requests_drawn": len(reqs), "wall_cap_s": wall_cap, "load": load,
+            "capacity_solves_per_s": cap, "policy": policy, "offered_solves_per_s": rate,
+            "solves_per_s": len(res) / wall, "wall_s": wall,
+            "p50_s": pct(lat, 50), "p99_s": pct(lat, 99), "p99_over_p50": pct(lat, 99) / pct(lat, 50),
+            "alone_p50_s": pct(svc, 50), "alone_p99_s": pct(svc, 99),
+            "alone_p99_over_p50": pct(svc, 99) / pct(svc, 50),
+            "slowdown_p50": pct(slow, 50), "slowdown_p99": pct(slow, 99),
+            "mean_photmax": float(np.mean([r.photmax for r in res])), "tolerance_met_frac": float(met.mean()),
             "gpu_busy_frac": (st1["busy_s"] - st0["busy_s"]) / wall, "hbm_in_use_gb": st1["hbm_in_use"] / 1e9,
-            "data": "synthetic",
+            "per_class": per_class,
             "config": {"workload": "Poisson stream, narrow-band 100x8, grids 32^3..256x128x128 in 8 log-spaced "
                                    "classes, tolerance 1-5% log-uniform, 150 GB budget",
-                       "classes": [[p.imax, p.jmax, p.kmax] for p, _ in classes],
-                       "max_inflight": args.serve_inflight}}
+                       "classes": [[p.imax, p.jmax, p.kmax] for p, _ in classes], "max_inflight": inflight}}
+
+
+def run_serve(args, rank, local):
+    """--serve: the serving run alone (no wall cap unless --serve-cap)."""
+    if rank != 0:
+        return
+    out = serve_run(local, args.serve_requests, args.load, args.serve_inflight, args.policy, args.serve_cap)
+    line = dict({"metric": "serve latency p50/p99 and solves/s", "impl": "ours", "n_gpus": 1, "data": "synthetic"},
+                **out)
     print(json.dumps(line), flush=True)
 
 
@@ -771,6 +828,14 @@ def run_ours(args, ws, rank, local):
         # 32/128), where one solve does not fill the GPU
         line["batched_small"] = leg_batched(dev, edges=(16, 24, 32), photmaxes=(32, 128))
         line["dns_source"] = leg_dns_source(dev, flush, cpu=not args.no_cpu_baseline)
+        # the same mixes at equal 1% relative std of max|Q| (photmax per
+        # problem from a pilot), one pass each
+        line["batched_at_1pct"] = leg_batched(dev, passes=1, tol=0.01, served=False, warm=False)
+        line["batched_small_at_1pct"] = leg_batched(dev, passes=1, tol=0.01, served=False, warm=False,
+                                                    edges=(16, 24, 32), photmaxes=(32, 128))
+        # serving: the open-loop Poisson stream at 80% load, bounded in wall
+        # time (requests submitted within the cap all complete)
+        line["serve"] = serve_run(dev, 200, 0.8, wall_cap=args.serve_leg_cap)
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         cb = cpu_sample(p, tabs, T, seconds=args.ref_seconds)
         line["cpu_baseline"] = {"value": cb["bundles"] / cb["seconds"], "unit": "bundles/s",
@@ -794,7 +859,7 @@ def main():
     ap.add_argument("--occupancy", type=int, default=0)
     ap.add_argument("--sort", type=int, default=-1, help="band-sorted bundle order 0/1 (default: context's)")
     ap.add_argument("--prio", type=float, default=None,
-                    help="long-ray priority threshold on |s_x| (0: off; default: context's)")
+                    help="long-ray priority: path-length threshold in channel widths (0: off; default: context's)")
     ap.add_argument("--ref-seconds", dest="ref_seconds", type=float, default=12.0)
     ap.add_argument("--traffic", type=float, default=None)
     ap.add_argument("--photmax", type=int, default=0, help="override bundles per cell (profiling runs)")
@@ -807,6 +872,10 @@ def main():
                     help="only the DNS coupling leg (profiling runs)")
     ap.add_argument("--serve-requests", dest="serve_requests", type=int, default=200)
     ap.add_argument("--serve-inflight", dest="serve_inflight", type=int, default=32)
+    ap.add_argument("--serve-leg-cap", dest="serve_leg_cap", type=float, default=60.0,
+                    help="wall-time cap of the default run's serving leg (s)")
+    ap.add_argument("--serve-cap", dest="serve_cap", type=float, default=None,
+                    help="no new request after this many seconds (serving run)")
     ap.add_argument("--policy", default="srpt", choices=["srpt", "fair"])
     ap.add_argument("--load", type=float, default=0.8)
     ap.add_argument("--ref-cuda-child", dest="ref_cuda_child", nargs=3, default=None,

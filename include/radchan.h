@@ -215,19 +215,26 @@ int rc_solve_info_get(rc_ctx *ctx, rc_ticket ticket, rc_solve_info *info);
  * allow (2, 3 or 4).  None of them changes which bundles are traced. */
 int rc_set_launch(rc_ctx *ctx, int rays_per_thread, int block_threads, int sort_bands, int occupancy);
 int rc_get_launch(rc_ctx *ctx, int *rays_per_thread, int *block_threads, int *sort_bands, int *occupancy);
-/* Long-ray priority of rc_solve_async / rc_solve_device_async (default
- * 4e-3; 0 turns it off).  A bundle emitted with |s_x| below the threshold,
- * nearly parallel to the x walls, can cross the periodic y/z boundaries
- * for up to the last level's step budget in a near-transparent band.  Such
- * a ray started late in a launch keeps the GPU waiting for it alone.
- * Before the march, a short pass draws every bundle's direction and the
- * tiles holding such a bundle are marched first.  It changes the order of
- * the work, never a result.  The list depends on the seed, photmax,
- * rays_per_thread, replicates and decomposition but not on T, so each solve
- * slot builds it once and reuses it while those stay the same.  It is used
- * only when no other solve of the context is still running on the device
- * (that solve fills the tail anyway), and solves of more than 2^22 tiles
- * skip it (there, reordering cost more than the tail it removed). */
+/* Long-ray priority of rc_solve_async / rc_solve_device_async.  A bundle
+ * whose path is long -- nearly parallel to the x walls, so that it crosses
+ * the periodic y/z boundaries again and again, and in a near-transparent
+ * band and g point -- takes up to the last level's step budget, and when it
+ * starts late in a launch the GPU waits for it alone.  Before the march a
+ * short pass draws every bundle's direction, band and g point exactly as
+ * emission will, estimates its path length as min(d_x / |s_x|,
+ * ln(1/tol) / k_min) (d_x the distance to the x wall it heads for, k_min the
+ * smallest k of its band and g point over the table rows the field spans)
+ * and lists the tiles holding a bundle whose estimate exceeds `threshold`
+ * channel widths Lx; the march claims those tiles first.  Default
+ * RC_PRIORITY_DEFAULT; 0 turns it off.  It changes the order of the work,
+ * never a result.  Each solve slot builds the list on its first solve and
+ * reuses it while the draws and the work decomposition stay the same (seed,
+ * photmax, rays_per_thread, replicates, grid, walls, threshold): a later
+ * field can only make the order less apt.  It is used only when no other
+ * solve of the context is still running on the device (that solve fills
+ * the tail anyway), and solves of more than 2^22 tiles skip it (there,
+ * reordering cost more than the tail it removed). */
+#define RC_PRIORITY_DEFAULT 12.0f
 int rc_set_priority(rc_ctx *ctx, float threshold);
 /* Try launch configurations on T (host) with a reduced bundle count
  * (pilot_photmax; <= 0: the context's photmax) and keep the fastest:
@@ -352,8 +359,10 @@ int rc_server_submit(rc_server *s, const rc_request *req, int64_t *id);
 int rc_server_wait(rc_server *s, int64_t id, float *Q, float *sigma, rc_result_info *info);
 int rc_server_stats(rc_server *s, double *solves, double *busy_s, double *hbm_in_use);
 /* Tiles (32 work items each) per march launch, shared among the running
- * requests (default 131072): smaller quanta let new requests start sooner,
- * larger ones cost fewer launches. */
+ * requests: smaller quanta let new requests start sooner, larger ones cost
+ * fewer launches.  0 (the default) sizes each quantum from the backlog: a
+ * 32nd of the running requests' remaining tiles, between 131072 and
+ * 524288. */
 int rc_server_set_quantum(rc_server *s, long long tiles);
 /* March launches issued so far. */
 int rc_server_quanta(rc_server *s, long long *quanta);

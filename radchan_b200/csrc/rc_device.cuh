@@ -39,7 +39,7 @@ namespace rc {
 constexpr int kWarp = 32;
 constexpr int kRing = 64;    // per-warp ring of emitted bundles (two waves)
 constexpr int kGuide = 256;  // buckets of the band-CDF guide tables
-constexpr int kFeedIdle = 8; // idle lanes that make a warp leave its step loop to take new bundles
+constexpr int kFeedIdle = 14; // idle lanes that make a warp leave its step loop to take new bundles
 constexpr int kChunkMax = 8;  // tiles a warp claims per work-queue fetch (guided: fewer near the end)
 
 // ---------------------------------------------------------------------------
@@ -285,12 +285,11 @@ __device__ __forceinline__ void select_band_g(const DSolve<R> &S, int kind, R u_
 // A bundle after emission, placed at its start point: position, cell,
 // direction, sampled band/g and OERM weights.
 template <typename R>
-struct Emitted {
-    R xp, yp, zp, sx, sy, sz, ratioI, invTi4;
-    int ij;    // ic | jc << 16
-    int kk;    // kc | kind << 16
+struct alignas(16) Emitted {
+    R sx, sy, sz, ratioI, invTi4;
+    int ij;    // ic | jc << 16: the emitting cell (fluid) or wall cell
+    int kk;    // kc | kind << 16 | pool index << 18 | pool parity << 29
     int nbg;   // nb | g << 20
-    int b;     // index in the warp's bundle pool
 };
 
 template <typename R>
@@ -302,7 +301,6 @@ struct Ray {
     R Ibmax, ratioI, invTi4, tol;
     const KIRow<R> *kicol;
     int ic, jc, kc;
-    int fx, fy, fz;
     int lev, counter;
     int nb;
     double De;
@@ -339,8 +337,6 @@ __device__ __forceinline__ bool emit_bundle(Emitted<R> &e, const DSolve<R> &S, i
     int Pi;
     int nb, g, ic = i;
     R st;
-    e.yp = S.yc[RC_IX(j, S.jmax + 2, SITE_CENTRE, S)];
-    e.zp = S.zc[RC_IX(k, S.kmax + 2, SITE_CENTRE, S)];
     if (kind == 0) {
         // isotropic: cos(theta) = 1 - 2u (emiss_ang, :1077-1084)
         const R mu = (R)1 - (R)2 * u_mu;
@@ -349,7 +345,6 @@ __device__ __forceinline__ bool emit_bundle(Emitted<R> &e, const DSolve<R> &S, i
         select_band_g(S, 0, u_b, u_g, nb, g);
         const DLevel<R> &L0 = S.lev[0];
         Pi = L0.P[RC_IX(cell_index(i, j, k, L0.im, L0.jm), (long long)L0.im * L0.jm * L0.km, SITE_EMIT_T, S)];
-        e.xp = S.xc[RC_IX(i, S.imax + 2, SITE_CENTRE, S)];
     } else {
         // Lambertian: theta = acos(1 - 2u)/2 (+pi/2 on the east wall)
         // (emiss_angS, :1093-1102), i.e. cos = sqrt(1-u) / -sqrt(u).
@@ -364,7 +359,6 @@ __device__ __forceinline__ bool emit_bundle(Emitted<R> &e, const DSolve<R> &S, i
         select_band_g(S, kind, u_b, u_g, nb, g);
         Pi = S.Pw0[bound][RC_IX((k - 1) * S.jmax + (j - 1), (long long)S.kmax * S.jmax, SITE_WALL_EMIT_T, S)];
         ic = (bound == 0) ? 1 : S.imax;
-        e.xp = (bound == 0) ? (R)0 : S.Lx;
     }
     e.sy = st * cp;
     e.sz = st * sp;
@@ -379,20 +373,8 @@ __device__ __forceinline__ bool emit_bundle(Emitted<R> &e, const DSolve<R> &S, i
         if (RT<R>::fabs_(e.sz) <= (R)1e-10) e.sz = (R)((e.sz > (R)0) - (e.sz <= (R)0)) * (R)1e-10;
     }
     e.nbg = nb | (g << 20);
-    int jc = j, kc = k;
-    if (kind != 0) {
-        // cell shift when the start point lies on a face (:1429-1441)
-        const DLevel<R> &G = S.lev[0];
-        const bool fx = e.sx < (R)0, fy = e.sy < (R)0, fz = e.sz < (R)0;
-        if (fx && e.xp == G.xu[RC_IX(ic - 1, G.im + 1, SITE_FACE_SHIFT, S)]) ic = ic - 1;
-        if (fy && e.yp == G.yu[RC_IX(jc - 1, G.jm + 1, SITE_FACE_SHIFT, S)]) jc = jc - 1;
-        if (fz && e.zp == G.zu[RC_IX(kc - 1, G.km + 1, SITE_FACE_SHIFT, S)]) kc = kc - 1;
-        if (!fx && e.xp == G.xu[RC_IX(ic, G.im + 1, SITE_FACE_SHIFT, S)]) ic = ic + 1;
-        if (!fy && e.yp == G.yu[RC_IX(jc, G.jm + 1, SITE_FACE_SHIFT, S)]) jc = jc + 1;
-        if (!fz && e.zp == G.zu[RC_IX(kc, G.km + 1, SITE_FACE_SHIFT, S)]) kc = kc + 1;
-    }
-    e.ij = ic | (jc << 16);
-    e.kk = kc | (kind << 16);
+    e.ij = ic | (j << 16);
+    e.kk = k | (kind << 16);
     // OERM weights
     const KIRow<R> row =
         S.ki[RC_IX(((size_t)nb * S.nQ + g) * S.nT + (Pi >> 8), (long long)S.nB * S.nQ * S.nT, SITE_EMIT_ROW, S)];
@@ -416,9 +398,25 @@ __device__ __forceinline__ bool emit_bundle(Emitted<R> &e, const DSolve<R> &S, i
 // Ray state of an emitted bundle.
 template <typename R>
 __device__ __forceinline__ void place_bundle(Ray<R> &r, const DSolve<R> &S, const Emitted<R> &e) {
-    r.xp = e.xp;
-    r.yp = e.yp;
-    r.zp = e.zp;
+    const int kind = (e.kk >> 16) & 3;
+    int ic = e.ij & 0xffff, jc = e.ij >> 16, kc = e.kk & 0xffff;
+    // start point: the cell centre, or the wall cell's point on the wall
+    // (kernel_fluid :117-122, kernel_surface :1381-1384)
+    r.xp = kind == 0 ? S.xc[RC_IX(ic, S.imax + 2, SITE_CENTRE, S)] : (kind == 1 ? (R)0 : S.Lx);
+    r.yp = S.yc[RC_IX(jc, S.jmax + 2, SITE_CENTRE, S)];
+    r.zp = S.zc[RC_IX(kc, S.kmax + 2, SITE_CENTRE, S)];
+    if (kind != 0) {
+        // cell shift when the start point lies on a face (:1429-1441)
+        const DLevel<R> &G = S.lev[0];
+        const bool fx = e.sx < (R)0, fy = e.sy < (R)0, fz = e.sz < (R)0;
+        const int i0 = ic, j0 = jc, k0 = kc;
+        if (fx && r.xp == G.xu[RC_IX(i0 - 1, G.im + 1, SITE_FACE_SHIFT, S)]) ic = i0 - 1;
+        if (fy && r.yp == G.yu[RC_IX(j0 - 1, G.jm + 1, SITE_FACE_SHIFT, S)]) jc = j0 - 1;
+        if (fz && r.zp == G.zu[RC_IX(k0 - 1, G.km + 1, SITE_FACE_SHIFT, S)]) kc = k0 - 1;
+        if (!fx && r.xp == G.xu[RC_IX(ic, G.im + 1, SITE_FACE_SHIFT, S)]) ic = ic + 1;
+        if (!fy && r.yp == G.yu[RC_IX(jc, G.jm + 1, SITE_FACE_SHIFT, S)]) jc = jc + 1;
+        if (!fz && r.zp == G.zu[RC_IX(kc, G.km + 1, SITE_FACE_SHIFT, S)]) kc = kc + 1;
+    }
     r.sx = e.sx;
     r.sy = e.sy;
     r.sz = e.sz;
@@ -430,13 +428,9 @@ __device__ __forceinline__ void place_bundle(Ray<R> &r, const DSolve<R> &S, cons
     const int nb = e.nbg & 0xfffff, g = e.nbg >> 20;
     r.nb = nb;
     r.kicol = S.ki + ((size_t)nb * S.nQ + g) * S.nT;
-    r.fx = r.sx < (R)0;
-    r.fy = r.sy < (R)0;
-    r.fz = r.sz < (R)0;
-    r.ic = e.ij & 0xffff;
-    r.jc = e.ij >> 16;
-    r.kc = e.kk & 0xffff;
-    const int kind = e.kk >> 16;
+    r.ic = ic;
+    r.jc = jc;
+    r.kc = kc;
     r.lev = 0;
     r.counter = 0;
     r.tra = (R)1;
@@ -484,12 +478,12 @@ __device__ __forceinline__ void hit_wall(Ray<R> &r, const DSolve<R> &S, const DL
         wall_deposit(r, RT<R>::lerp_(row.ib0, row.ib1, fr));
     } else if (t == 3) {  // specular
         switch (w) {
-            case RC_WEST: r.xp = (R)0; r.sx = -r.sx; r.isx = -r.isx; r.ic = 1; r.fx = r.sx < (R)0; break;
-            case RC_EAST: r.xp = S.Lx; r.sx = -r.sx; r.isx = -r.isx; r.ic = L.im; r.fx = r.sx < (R)0; break;
-            case RC_SOUTH: r.yp = (R)0; r.sy = -r.sy; r.isy = -r.isy; r.jc = 1; r.fy = r.sy < (R)0; break;
-            case RC_NORTH: r.yp = S.Ly; r.sy = -r.sy; r.isy = -r.isy; r.jc = L.jm; r.fy = r.sy < (R)0; break;
-            case RC_BOT: r.zp = (R)0; r.sz = -r.sz; r.isz = -r.isz; r.kc = 1; r.fz = r.sz < (R)0; break;
-            default: r.zp = S.Lz; r.sz = -r.sz; r.isz = -r.isz; r.kc = L.km; r.fz = r.sz < (R)0; break;
+            case RC_WEST: r.xp = (R)0; r.sx = -r.sx; r.isx = -r.isx; r.ic = 1; break;
+            case RC_EAST: r.xp = S.Lx; r.sx = -r.sx; r.isx = -r.isx; r.ic = L.im; break;
+            case RC_SOUTH: r.yp = (R)0; r.sy = -r.sy; r.isy = -r.isy; r.jc = 1; break;
+            case RC_NORTH: r.yp = S.Ly; r.sy = -r.sy; r.isy = -r.isy; r.jc = L.jm; break;
+            case RC_BOT: r.zp = (R)0; r.sz = -r.sz; r.isz = -r.isz; r.kc = 1; break;
+            default: r.zp = S.Lz; r.sz = -r.sz; r.isz = -r.isz; r.kc = L.km; break;
         }
     } else {  // lost ray
         r.tra = (R)0;
@@ -497,15 +491,18 @@ __device__ __forceinline__ void hit_wall(Ray<R> &r, const DSolve<R> &S, const DL
 }
 
 // One ray-cell crossing (one iteration of the while loop of march_ray,
-// :252-656).
+// :252-656).  Returns the step budget (maxs) of the level the step was
+// taken on, which the caller compares with the step counter.  The side of
+// the cell a ray leaves through on each axis follows from the sign of its
+// direction component (never 0: emission floors it at 1e-10).
 template <typename R>
-__device__ __forceinline__ void march_step(Ray<R> &r, const DSolve<R> &S) {
+__device__ __forceinline__ int march_step(Ray<R> &r, const DSolve<R> &S) {
     // S lives in global memory (read-only during every kernel that steps)
     const int4 A = __ldg(&S.lva[RC_IX(r.lev, S.nlev, SITE_LEVEL, S)]);
     const int4 B = __ldg(&S.lvb[RC_IX(r.lev, S.nlev, SITE_LEVEL, S)]);
-    const R fxu = __ldg(S.faces + RC_IX(A.x + r.ic - r.fx, S.n_faces, SITE_FACE, S));
-    const R fyu = __ldg(S.faces + RC_IX(A.y + r.jc - r.fy, S.n_faces, SITE_FACE, S));
-    const R fzu = __ldg(S.faces + RC_IX(A.z + r.kc - r.fz, S.n_faces, SITE_FACE, S));
+    const R fxu = __ldg(S.faces + RC_IX(A.x + r.ic - (int)(r.sx < (R)0), S.n_faces, SITE_FACE, S));
+    const R fyu = __ldg(S.faces + RC_IX(A.y + r.jc - (int)(r.sy < (R)0), S.n_faces, SITE_FACE, S));
+    const R fzu = __ldg(S.faces + RC_IX(A.z + r.kc - (int)(r.sz < (R)0), S.n_faces, SITE_FACE, S));
 #if RC_CHECKED
     // the cell itself must lie inside its level (a face index alone can be
     // in the shared faces array while the cell is off its level)
@@ -543,7 +540,7 @@ __device__ __forceinline__ void march_step(Ray<R> &r, const DSolve<R> &S) {
     // crossed axis (ties: x only if strictly smallest, :375-377, 524)
     const int axis = (dsx < dsy) ? ((dsx < dsz) ? 0 : 2) : ((dsy < dsz) ? 1 : 2);
     const bool ax0 = axis == 0, ax1 = axis == 1;
-    const int f = ax0 ? r.fx : (ax1 ? r.fy : r.fz);
+    const bool f = ax0 ? (r.sx < (R)0) : (ax1 ? (r.sy < (R)0) : (r.sz < (R)0));
     const int dlt = f ? -1 : 1;
     r.ic += ax0 ? dlt : 0;
     r.jc += ax1 ? dlt : 0;
@@ -572,6 +569,7 @@ __device__ __forceinline__ void march_step(Ray<R> &r, const DSolve<R> &S) {
         }
     }
     r.counter += 1;
+    return B.w;
 }
 
 // Index of the coarse cell holding fine cell n (1-based): (n + r - 1) / r,

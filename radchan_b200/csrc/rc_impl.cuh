@@ -168,11 +168,17 @@ struct SlotCommon {
     long long *d_tiles = nullptr, *h_tiles = nullptr;
     unsigned long long *d_counter = nullptr;
     TallyOut *d_out = nullptr, *h_out = nullptr;
-    // long-ray priority list (k_prio_tiles): listed tiles, per-tile flag, count
+    // long-ray priority list (k_prio_tiles): listed tiles, per-tile flag,
+    // count, and the smallest k of every band and g point over the field's
+    // temperature range (k_prio_kmin)
     unsigned *d_prio = nullptr, *d_nprio = nullptr;
     unsigned char *d_tprio = nullptr;
+    float *d_kmin = nullptr;
     long long prio_cap = 0;
-    // what the list was built for (it does not depend on the field)
+    int kmin_cap = 0;
+    // what the list was built for: the work decomposition and the draws; the
+    // list is kept while those stay the same (a later field only changes how
+    // well it orders the work, never a result)
     long long prio_key[10] = {};
     bool prio_ok = false;
     int state = 0;  // 0 free, 1 in flight, 2 finished (results pending)
@@ -194,7 +200,7 @@ struct rc_ctx {
     int next_ticket = 1;
     // launch knobs
     int rpt = 8, block = 256, sort = 0, minb = 3;
-    float prio_thr = 4e-3f;  // long-ray priority: |s_x| below this marks a tile (0: off)
+    float prio_thr = RC_PRIORITY_DEFAULT;  // long-ray priority: estimated path length in units of Lx (0: off)
     int num_sms = 148;
     bool has_tables = false;
     // DNS-coupling scratch (rc_dns_source): T1 pencil + four outputs, and a counter
@@ -295,7 +301,9 @@ struct Impl : ImplBase {
             dfree(s.d_prio);
             dfree(s.d_tprio);
             dfree(s.d_nprio);
+            dfree(s.d_kmin);
             s.prio_cap = 0;
+            s.kmin_cap = 0;
             s.prio_ok = false;
             dfree(s.d_levAll);
             s.d_levT.clear();
@@ -781,17 +789,18 @@ struct Impl : ImplBase {
         return minb <= 2 ? k_march<R, 2> : minb == 3 ? k_march<R, 3> : k_march<R, 4>;
     }
 
-    // Long-ray priority list of a one-solve launch (k_prio_tiles) on stream
-    // st, into the slot's buffers; `use` stays false when the knob is off or
-    // the solve has more tiles than the list is kept for (its tail is then
-    // a small share of the launch).  The list depends only on the bundles'
-    // directions, i.e. on the seed, photmax, rays_per_thread, replicates and
-    // the work decomposition -- never on the temperature field -- so the
-    // slot keeps it and rebuilds it only when one of those changes.
-    // The tail it removes is a fixed few ms per launch (the longest rays),
-    // while reordering costs in proportion to the work: on the 64^3
-    // narrow-band channel it saved 3.9 ms at 2.1 M tiles (photmax 256) and
-    // lost 4 ms at 4.3 M tiles (photmax 512).
+    // Long-ray priority list of a one-solve launch (k_prio_kmin +
+    // k_prio_tiles) on stream st, into the slot's buffers; `use` stays false
+    // when the knob is off or the solve has more tiles than the list is kept
+    // for (its tail is then a small share of the launch).  The list is built
+    // from the bundles' own draws, band CDF and temperature range of the
+    // solve it is first built for, and kept while the draws and the work
+    // decomposition stay the same (seed, photmax, rays_per_thread,
+    // replicates, grid, walls, threshold): a DNS calling with one parameter
+    // set every radStep pays for it once, and a later field can only make the
+    // order less apt, never change a result.  The tail it removes is a fixed
+    // few ms per launch (the longest rays), while reordering costs pyramid
+    // locality in proportion to the work, hence the limit on tiles.
     static constexpr long long kPrioMaxTiles = 1LL << 22;
     int enqueue_prio(Slot<R> &s, cudaStream_t st, bool &use) {
         std::string *err_ = &c->err;
@@ -819,10 +828,20 @@ struct Impl : ImplBase {
             RC_CK(cudaMalloc((void **)&s.d_tprio, nt));
             s.prio_cap = nt;
         }
+        const int nbq = d.nB * d.nQ;
+        if (s.kmin_cap < nbq) {
+            dfree(s.d_kmin);
+            s.kmin_cap = 0;
+            RC_CK(cudaMalloc((void **)&s.d_kmin, nbq * sizeof(float)));
+            s.kmin_cap = nbq;
+        }
         if (!s.d_nprio) RC_CK(cudaMalloc((void **)&s.d_nprio, sizeof(unsigned)));
         RC_CK(cudaMemsetAsync(s.d_nprio, 0, sizeof(unsigned), st));
+        k_prio_kmin<R><<<(nbq + 255) / 256, 256, 0, st>>>(s.d_desc, s.d_kmin);
+        RC_CK(cudaGetLastError());
         const long long grid = std::max<long long>(1, std::min<long long>((nt + 7) / 8, (long long)c->num_sms * 16));
-        k_prio_tiles<R><<<(unsigned)grid, 256, 0, st>>>(s.d_desc, (R)c->prio_thr, s.d_prio, s.d_tprio, s.d_nprio);
+        k_prio_tiles<R><<<(unsigned)grid, 256, 0, st>>>(s.d_desc, c->prio_thr, s.d_kmin, s.d_prio, s.d_tprio,
+                                                         s.d_nprio);
         RC_CK(cudaGetLastError());
         memcpy(s.prio_key, key, sizeof(key));
         s.prio_ok = true;

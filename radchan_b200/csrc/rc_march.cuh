@@ -27,10 +27,12 @@ namespace rc {
 //     tile's last bundle has finished, its slots are summed in bundle
 //     order, so the result does not depend on which lane traced which
 //     bundle.
-// Shared memory per warp is the ring (64 emitted bundles) and two slot
-// arrays; everything else stays in L1-cached global memory, so that most of
-// the SM's 256 KB of L1/shared storage caches the temperature pyramid and
-// the k / I_b tables.
+// Shared memory per warp is the ring (64 emitted bundles of 32 bytes: the
+// start position is rebuilt from the emitting cell when a lane takes the
+// bundle) and two slot arrays; everything else stays in L1-cached global
+// memory, so that most of the SM's 256 KB of L1/shared storage caches the
+// temperature pyramid and the k / I_b tables (48-byte entries, the
+// round-1 layout, were 1.2% slower; 64-byte entries 4%).
 
 struct MarchArgs {
     const void *solves;          // DSolve<R>[nsolves] (run-time fields patched on the device)
@@ -47,21 +49,42 @@ struct MarchArgs {
     const unsigned *n_prio;
 };
 
-// Tiles holding a bundle emitted within `thr` of the x-wall planes
-// (|s_x| < thr): in a near-transparent band such a ray runs between the
-// periodic y/z boundaries for up to the last level's step budget, so a
-// launch that meets it late idles while it finishes.  One warp per tile
-// draws the same direction uniform as the emission (Philox counter of the
-// bundle, emit_bundle) for each of the tile's bundles; tiles with a
-// candidate are listed (in any order) and flagged.  Only the order in which
-// tiles are claimed changes, never a result.
+// Long-ray priority list.  A bundle whose path is long -- nearly parallel
+// to the x walls, so that it runs between the periodic y/z boundaries, and
+// in a near-transparent band, so that its transmissivity stays above the
+// cutoff -- takes up to the last level's step budget; a launch that starts
+// it late idles while it finishes.  The march therefore claims the tiles
+// holding such a bundle first.  The estimate of a bundle's path length is
+//   L = min(d_x / |s_x|, ln(1/tol) / k_min),
+// d_x the distance from its start to the x wall it moves towards, k_min the
+// smallest absorption coefficient of its band and g point over the table
+// rows the field's temperatures span (k_prio_kmin); a tile is listed when
+// some bundle has L > thr * Lx.  The draws are the emission's own (Philox
+// counter of the bundle, select_band_g), so the estimate sees the same
+// direction, band and g point the march will trace.  Only the order in
+// which tiles are claimed changes, never a result.
 template <typename R>
-__global__ void k_prio_tiles(const DSolve<R> *Sp, R thr, unsigned *prio_tiles, unsigned char *tile_prio,
-                             unsigned *n_prio) {
+__global__ void k_prio_kmin(const DSolve<R> *Sp, float *kmin) {
+    const DSolve<R> &S = *Sp;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= S.nB * S.nQ) return;
+    const double T0 = S.sc->T0, idt = S.sc->inv_dT;
+    const double tmin = (double)__uint_as_float(S.sc->tmin_bits), tmax = (double)__uint_as_float(S.sc->tmax_bits);
+    const int lo = max(0, min(S.nT - 1, (int)floor((tmin - T0) * idt)));
+    const int hi = max(lo, min(S.nT - 1, (int)floor((tmax - T0) * idt) + 1));
+    float k = 3.0e38f;
+    for (int t = lo; t <= hi; ++t) k = fminf(k, (float)S.ki[(size_t)i * S.nT + t].k0);
+    kmin[i] = fmaxf(k, 0.f);
+}
+
+template <typename R>
+__global__ void k_prio_tiles(const DSolve<R> *Sp, float thr, const float *kmin, unsigned *prio_tiles,
+                             unsigned char *tile_prio, unsigned *n_prio) {
     const DSolve<R> &S = *Sp;
     const int lane = threadIdx.x & 31;
     const long long nw = (long long)gridDim.x * (blockDim.x >> 5);
-    const R thr2 = thr * thr;
+    const float Lx = (float)S.Lx, Lthr = thr * Lx;
+    const float tau_f = logf(1.0f / fmaxf((float)S.toll, 1e-30f)), tau_w = logf(1.0f / fmaxf((float)S.tollS, 1e-30f));
     for (long long tile = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); tile < S.n_tiles;
          tile += nw) {
         const ItemId it = decode_item(S, tile * kWarp + lane);
@@ -70,13 +93,21 @@ __global__ void k_prio_tiles(const DSolve<R> *Sp, R thr, unsigned *prio_tiles, u
             const uint32_t cell = (it.kind == 0)
                                       ? (uint32_t)((it.i - 1) + S.imax * ((it.j - 1) + S.jmax * (it.k - 1)))
                                       : (uint32_t)((it.j - 1) + S.jmax * (it.k - 1));
+            const float x0 = it.kind == 0 ? (float)S.xc[it.i] : (it.kind == 1 ? 0.f : Lx);
+            const float tau = it.kind == 0 ? tau_f : tau_w;
             const int h1 = min(it.h0 + S.rpt, S.photmax);
-            for (int h = it.h0; h < h1; ++h) {
+            for (int h = it.h0; h < h1 && !cand; ++h) {
                 const rc_u32x4 d = bundle_draws(S.key0, S.key1, h, it.v, it.kind, cell);
-                const R u = (R)rc_u01(d.y);
-                if (it.kind == 0) cand = cand || RT<R>::fabs_((R)1 - (R)2 * u) < thr;  // s_x = 1 - 2u
-                else if (it.kind == 1) cand = cand || (R)1 - u < thr2;                 // s_x = sqrt(1 - u)
-                else cand = cand || u < thr2;                                           // s_x = -sqrt(u)
+                const float u = rc_u01(d.y);
+                // s_x as emit_bundle draws it: 1 - 2u (fluid), sqrt(1 - u) / -sqrt(u) (walls)
+                const float sx = it.kind == 0 ? 1.f - 2.f * u : (it.kind == 1 ? sqrtf(1.f - u) : -sqrtf(u));
+                const float dx = sx > 0.f ? Lx - x0 : x0;
+                const float Lw = dx / fmaxf(fabsf(sx), 1e-10f);
+                if (!(Lw > Lthr)) continue;
+                int nb, g;
+                select_band_g(S, it.kind, (R)rc_u01(d.z), (R)rc_u01(d.w), nb, g);
+                const float k = kmin[nb * S.nQ + g];
+                cand = k * Lthr < tau;  // ln(1/tol) / k > Lthr
             }
         }
         const unsigned m = __ballot_sync(0xffffffffu, cand);
@@ -245,7 +276,7 @@ __global__ void __launch_bounds__(256, MINB) k_march(MarchArgs a) {
                 if (it.kind >= 0 && h < S.photmax) {
                     nbund++;
                     ok = emit_bundle(e, S, it.kind, it.i, it.j, it.k, it.v, h);
-                    e.b = b | (epar << 16);
+                    e.kk |= (b << 18) | (epar << 29);
                 }
             }
             const unsigned m = __ballot_sync(0xffffffffu, ok);
@@ -288,8 +319,8 @@ __global__ void __launch_bounds__(256, MINB) k_march(MarchArgs a) {
                 if (rank < navail) {
                     const Emitted<R> &e = ws->ring[(head + rank) & (kRing - 1)];
                     place_bundle(r, S, e);
-                    myb = e.b & 0xffff;
-                    mypar = e.b >> 16;
+                    myb = (e.kk >> 18) & 0x7ff;
+                    mypar = (e.kk >> 29) & 1;
                     took = true;
                     active = level_advance(r, S);
                     if (!active) {
@@ -321,10 +352,10 @@ __global__ void __launch_bounds__(256, MINB) k_march(MarchArgs a) {
             for (;;) {
                 bool fin = false;
                 if (active) {
-                    march_step(r, S);
+                    const int budget = march_step(r, S);
                     nsteps++;
                     bool done = !(r.tra > r.tol);
-                    if (!done) done = !level_advance(r, S);
+                    if (!done && r.counter >= budget) done = !level_advance(r, S);
                     if (done) {
                         slots0[mypar * pool_max + myb] = r.De;
                         active = false;

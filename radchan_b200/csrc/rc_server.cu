@@ -83,7 +83,13 @@ struct PoolCtx {
     bool busy;
 };
 
-constexpr long long kQuantumTiles = 131072;  // default quantum: 16.8M bundles at 4 rays per thread
+// Quantum size when none is set: a 32nd of the running requests' remaining
+// tiles, between kQuantumTiles (16.8M bundles at 4 rays per thread, about
+// 2 ms of march) and kQuantumMax.  Small backlogs keep quanta short, so a new
+// request joins the device soon; a large backlog (many solves submitted at
+// once) pays fewer quantum preludes and tails per solve.
+constexpr long long kQuantumTiles = 131072;
+constexpr long long kQuantumMax = 4 * kQuantumTiles;
 constexpr long long kMinShare = 4096;
 constexpr int kPilotPhotmax = 64;
 constexpr int kMaxPhotmax = 1 << 20;
@@ -94,7 +100,7 @@ struct rc_server {
     int device = 0;
     double budget = 0;
     int max_inflight = 8;
-    long long quantum_tiles = kQuantumTiles;
+    long long quantum_tiles = 0;  // 0: sized from the backlog (kQuantumTiles .. kQuantumMax)
     int policy = RC_SCHED_SRPT;
     long long quanta = 0;
     std::vector<std::unique_ptr<TableSet>> tables;  // stable addresses: appended while the worker reads
@@ -363,6 +369,11 @@ int run_quantum(rc_server *sv, const std::vector<SrvReq *> &marching, int par) {
         qt = sv->quantum_tiles;
         policy = sv->policy;
         sv->quanta++;
+    }
+    if (qt <= 0) {
+        long long backlog = 0;
+        for (int i = 0; i < n; ++i) backlog += marching[i]->tiles - marching[i]->next_tile;
+        qt = std::min(kQuantumMax, std::max(kQuantumTiles, backlog / 32));
     }
     std::vector<long long> take(n, 0);
     if (policy == RC_SCHED_FAIR) {
@@ -783,7 +794,7 @@ int rc_server_cancel(rc_server *sv, int64_t id) {
 
 int rc_server_set_quantum(rc_server *sv, long long tiles) {
     if (!sv) return set_err(nullptr, RC_E_INVALID, "NULL server");
-    if (tiles < 1) return set_err(nullptr, RC_E_INVALID, "quantum must be >= 1 tile");
+    if (tiles < 0) return set_err(nullptr, RC_E_INVALID, "quantum must be >= 1 tile (0: sized from the backlog)");
     std::lock_guard<std::mutex> lk(sv->mu);
     sv->quantum_tiles = tiles;
     return RC_OK;

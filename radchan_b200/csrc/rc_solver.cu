@@ -225,7 +225,8 @@ int rc_set_launch(rc_ctx *c, int rays_per_thread, int block_threads, int sort_ba
 
 int rc_set_priority(rc_ctx *c, float threshold) {
     if (!c) return set_err(nullptr, RC_E_INVALID, "NULL context");
-    if (!(threshold >= 0.f) || threshold > 1.f) return set_err(&c->err, RC_E_INVALID, "threshold must be in [0, 1]");
+    if (!(threshold >= 0.f) || threshold > 1e9f)
+        return set_err(&c->err, RC_E_INVALID, "threshold must be a path length in [0, 1e9] channel widths");
     c->prio_thr = threshold;
     return RC_OK;
 }

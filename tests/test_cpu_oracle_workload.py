@@ -55,3 +55,14 @@ def test_reference_format_files_read_back_as_the_library_files(tmp_path):
     b = api.TableSet.read_dir(str(tmp_path / "l"), 32, 24, 4).arrays()
     for k in ("Tnb", "kP", "wvl", "wvr", "wvc", "kavg", "kq", "prob", "probg"):
         assert np.array_equal(a[k], b[k]), k
+
+
+def test_both_bench_arms_report_the_same_config():
+    import bench
+    for name in ("nb64", "grey32"):
+        po = bench.workload_oracle(name)[0]
+        pl = bench.workload(name)[0]
+        assert bytes(po) == bytes(pl)
+        for ws in (1, 4):
+            assert bench.bench_config(bench.workload_desc(name, po), ws) == \
+                bench.bench_config(bench.workload_desc(name, pl), ws)

@@ -39,9 +39,10 @@ def test_sort_block_occupancy_leave_result_unchanged(grey):
 
 @pytest.mark.parametrize("grey", [True, False])
 def test_long_ray_priority_changes_order_not_results(grey):
-    """Tiles with near-grazing bundles marched first (rc_set_priority): the
-    same bundles, steps and bit-identical results for any threshold, off
-    included, and equal to the oracle."""
+    """Tiles holding a long ray (estimated path above the threshold, in
+    channel widths Lx) marched first (rc_set_priority): the same bundles,
+    steps and bit-identical results for any threshold, off included, and
+    equal to the oracle."""
     from oracle import oracle as O
     if grey:
         p, tabs, T = W.config_grey_32(photmax=32), None, W.channel_field(W.config_grey_32(), seed=5)
@@ -49,15 +50,15 @@ def test_long_ray_priority_changes_order_not_results(grey):
         p, tabs, T = _nb_case()
     s = api.Solver(p, tabs)
     runs = []
-    # 4e-3 twice: the second solve reuses the slot's list (the list depends
-    # on the bundles' directions only); the field changes between them
-    for thr, T_ in ((0.0, T), (1e-3, T), (4e-3, T), (4e-3, T), (0.05, T), (1.0, T)):
+    # 100 twice: the second solve reuses the slot's list (kept while the
+    # draws and the decomposition stay the same)
+    for thr, T_ in ((0.0, T), (2.0, T), (100.0, T), (100.0, T), (20.0, T), (1e6, T)):
         s.set_priority(thr)
         t = s.solve_async(T_)
         i = s.info(t)
         runs.append((s.collect(t), i.bundles, i.steps))
     T2 = T * np.float32(1.02)
-    s.set_priority(4e-3)
+    s.set_priority(100.0)
     r2 = s.solve(T2)
     s.set_priority(0.0)
     np.testing.assert_array_equal(s.solve(T2).q64, r2.q64)
