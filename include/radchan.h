@@ -166,10 +166,77 @@ int rc_tables_validate(const rc_tables *t, char *msg, size_t msglen);
 int rc_tables_view(const rc_table_set *ts, rc_tables *view);
 void rc_tables_free(rc_table_set *ts);
 
+/* ---------------- scattering particles ---------------- */
+
+/* Scattering by suspended particles.  The reference's Monte Carlo path has
+ * no scattering; its table generator tabulates the particles: per band the
+ * absorption and scattering coefficients at each g point
+ * (nbcorrk/write_tables.cpp:204-260, writeP) and the cumulative
+ * phase-function probability over the scattering angle
+ * (nbcorrk/write_tables.cpp:326-336, writeH, built by
+ * nbcorrk/calc_prob.cpp:253-270).  Absorption by the particles belongs in
+ * the absorption tables (rc_tables); this adds their scattering.  Bands and
+ * g points are the context's (grey gas: grey_nB bands, nQ = 1). */
+typedef struct rc_scattering {
+    int nB, nQ, nA;
+    const float *ksca;       /* [nB][nQ] scattering coefficient (1/m; scaled by
+                                chanHeight on upload like k); no temperature axis */
+    const float *kabs;       /* [nB][nQ] particle absorption from the files, or
+                                NULL; informational (fold it into rc_tables) */
+    const float *theta;      /* [nA] scattering angles (radians), increasing from 0,
+                                at most pi */
+    const float *phase_cdf;  /* [nB][nA] cumulative probability of the scattering
+                                angle: 0 at theta[0], non-decreasing, 1 at theta[nA-1] */
+} rc_scattering;
+
+/* Seeded synthetic particle tables: Henyey-Greenstein phase function
+ * p(cos t) = (1 - g^2) / (1 + g^2 - 2 g cos t)^(3/2) per band with asymmetry
+ * g_b ~ U[g_lo, g_hi], tabulated at nA angles j pi / (nA - 1) and integrated
+ * as calc_prob.cpp:253-270 does (trapezoids of p sin t, normalised by the
+ * last); ksca_b ~ log-uniform on [ksca_lo, ksca_hi], the same at every g
+ * point; kabs 0. */
+typedef struct rc_scatter_spec {
+    int nB, nQ, nA;
+    double ksca_lo, ksca_hi;
+    double g_lo, g_hi;
+    uint64_t seed;
+} rc_scatter_spec;
+
+/* Host-owned particle table set. */
+typedef struct rc_scatter_set rc_scatter_set;
+
+int rc_scattering_synthetic(const rc_scatter_spec *spec, rc_scatter_set **out);
+/* Read dir/NarrBand%d.txt (writeP format: "wvl wvr wvc", then the nQ
+ * absorption and the nQ scattering coefficients) for nB bands and
+ * dir/prob_scatt.txt (writeH format: "theta wvc cdf" for every band and
+ * angle, angles fastest; nA is the row count over nB). */
+int rc_scattering_read_dir(const char *dir, int nB, int nQ, rc_scatter_set **out);
+int rc_scattering_write_dir(const rc_scatter_set *s, const char *dir);
+/* What the march assumes of particle tables: 1 <= nB, nQ; 2 <= nA <= 4096;
+ * ksca finite and >= 0; angles finite, strictly increasing, theta[0] >= 0,
+ * theta[nA-1] <= pi; every band's CDF finite, non-decreasing, 0 at the
+ * first angle and within 1e-6 of 1 at the last.  RC_E_INVALID with the
+ * first violation in msg otherwise.  Needs no GPU. */
+int rc_scattering_validate(const rc_scattering *s, char *msg, size_t msglen);
+/* Borrowed view (valid until rc_scattering_free). */
+int rc_scattering_view(const rc_scatter_set *s, rc_scattering *view);
+void rc_scattering_free(rc_scatter_set *s);
+
 /* ---------------- solver context ---------------- */
 
 int rc_create(const rc_params *p, int device, rc_ctx **out);
 int rc_set_tables(rc_ctx *ctx, const rc_tables *t);
+/* Particle scattering for the context's later solves (NULL removes it; no
+ * counterpart in the reference, whose medium only absorbs and emits).
+ * Bundles then travel a free path drawn against the scattering coefficient
+ * of their band and g point, turn by an angle drawn from the band's phase
+ * function and a uniform azimuth at each event, and keep absorbing along
+ * the way as before; every draw comes from the bundle's own Philox counter
+ * (emission's, with an event number), so results stay independent of the
+ * launch shape.  Batches run such contexts in the scattering variant of the
+ * march; the server serves media without scattering only.  Set it between
+ * solves (no solve of the context in flight). */
+int rc_set_scattering(rc_ctx *ctx, const rc_scattering *s);
 /* Copy T (host, whole field incl. ghosts) and launch; returns at once. */
 int rc_solve_async(rc_ctx *ctx, const float *T, int zstart, rc_ticket *ticket);
 /* Same with T already in device memory (same layout). */

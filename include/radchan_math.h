@@ -24,6 +24,9 @@
  *  - rc_sincos2pif: sin/cos of 2*pi*u by reduction to the nearest quarter
  *    turn and Taylor series on [-pi/4, pi/4].  Used for the azimuth of
  *    emitted bundles (mc_gpu_noint.cu:1079-1083).
+ *  - rc_logf/rc_log: natural logarithm by exponent extraction and the
+ *    atanh series 2 (s + s^3/3 + s^5/5 + ...), s = (m-1)/(m+1).  Used for the
+ *    free path -ln(u) between scattering events (optional particle media).
  *  - rc_planck: spectral blackbody intensity I_b(T, nu) with nu in cm^-1,
  *    restating I_blackC (src/montecarlo/memory_copy_noint.cu:288-297) in
  *    double precision with expm1 for the denominator.
@@ -62,6 +65,13 @@ RC_HD double rc_u64_as_f64(uint64_t u) {
     return __longlong_as_double((long long)u);
 #else
     double d; memcpy(&d, &u, 8); return d;
+#endif
+}
+RC_HD uint64_t rc_f64_as_u64(double d) {
+#if defined(__CUDA_ARCH__)
+    return (uint64_t)__double_as_longlong(d);
+#else
+    uint64_t u; memcpy(&u, &d, 8); return u;
 #endif
 }
 
@@ -227,6 +237,57 @@ RC_HD double rc_expm1(double x) {
 }
 
 /* ------------------------------------------------------------------ */
+/* natural logarithm                                                   */
+/* ------------------------------------------------------------------ */
+/* ln x for finite x > 0 in the normal range: x = m 2^e with m in
+ * [sqrt(1/2), sqrt(2)), ln x = e ln2 + 2 atanh(s) with s = (m-1)/(m+1),
+ * |s| <= 0.1716, and atanh(s) = s + s^3/3 + s^5/5 + ... (the series in
+ * powers of s^2, evaluated by Horner's rule).  m - 1 is exact (Sterbenz).
+ * Used for the free path -ln(u) between scattering events. */
+RC_HD float rc_logf(float x) {
+    uint32_t b = rc_f32_as_u32(x);
+    int e = (int)((b >> 23) & 0xffu) - 127;
+    float m = rc_u32_as_f32((b & 0x007fffffu) | 0x3f800000u);  /* [1, 2) */
+    if (m > 1.41421354f) { m = m * 0.5f; e = e + 1; }
+    float s = (m - 1.0f) / (m + 1.0f);
+    float s2 = s * s;
+    /* 2 atanh(s) = 2s (1 + s^2/3 + s^4/5 + s^6/7 + s^8/9); the first
+     * omitted term, s^10/11, is below 5e-9 relative */
+    float p = 1.1111111193895340e-01f;          /* 1/9 */
+    p = fmaf(p, s2, 1.4285714924335480e-01f);   /* 1/7 */
+    p = fmaf(p, s2, 2.0000000298023224e-01f);   /* 1/5 */
+    p = fmaf(p, s2, 3.3333334326744080e-01f);   /* 1/3 */
+    float t = 2.0f * s;
+    float l = fmaf(t * s2, p, t);
+    float fe = (float)e;
+    return fmaf(fe, RC_LN2_HI_F, fmaf(fe, RC_LN2_LO_F, l));
+}
+
+RC_HD double rc_log(double x) {
+    uint64_t b = rc_f64_as_u64(x);
+    int e = (int)((b >> 52) & 0x7ffu) - 1023;
+    double m = rc_u64_as_f64((b & 0x000fffffffffffffull) | 0x3ff0000000000000ull);
+    if (m > 1.4142135623730951) { m = m * 0.5; e = e + 1; }
+    double s = (m - 1.0) / (m + 1.0);
+    double s2 = s * s;
+    /* 2s (1 + s^2/3 + ... + s^20/21); first omitted term s^22/23 < 6e-19 */
+    double p = 4.7619047619047616e-02;        /* 1/21 */
+    p = fma(p, s2, 5.2631578947368418e-02);   /* 1/19 */
+    p = fma(p, s2, 5.8823529411764705e-02);   /* 1/17 */
+    p = fma(p, s2, 6.6666666666666666e-02);   /* 1/15 */
+    p = fma(p, s2, 7.6923076923076927e-02);   /* 1/13 */
+    p = fma(p, s2, 9.0909090909090912e-02);   /* 1/11 */
+    p = fma(p, s2, 1.1111111111111111e-01);   /* 1/9 */
+    p = fma(p, s2, 1.4285714285714285e-01);   /* 1/7 */
+    p = fma(p, s2, 2.0000000000000001e-01);   /* 1/5 */
+    p = fma(p, s2, 3.3333333333333331e-01);   /* 1/3 */
+    double t = 2.0 * s;
+    double l = fma(t * s2, p, t);
+    double fe = (double)e;
+    return fma(fe, RC_LN2_HI_D, fma(fe, RC_LN2_LO_D, l));
+}
+
+/* ------------------------------------------------------------------ */
 /* sin/cos of 2*pi*u                                                   */
 /* ------------------------------------------------------------------ */
 #define RC_TWO_PI_F 6.2831854820251465f
@@ -315,6 +376,20 @@ RC_HD double rc_planck(double T, double nu) {
     if (x > 700.0) return 0.0;
     double den = rc_expm1(x);
     return RC_PLANCK_C1 * eta * eta * eta / (RC_PI_D * den);
+}
+
+/* ------------------------------------------------------------------ */
+/* scattering table conversions (library and oracle alike)             */
+/* ------------------------------------------------------------------ */
+/* Scattering coefficient scaled by chanHeight as the reference scales k
+ * on load (read_tables.cpp:30,56), rounded to float. */
+RC_HD float rc_scatter_coef_scaled(float k, double chanHeight) {
+    return (float)((double)k * chanHeight);
+}
+/* A scattering angle in radians as turns (theta / 2 pi), rounded to float:
+ * the argument of rc_sincos2pif. */
+RC_HD float rc_angle_turns(float theta) {
+    return (float)((double)theta / (2.0 * RC_PI_D));
 }
 
 #endif /* RADCHAN_MATH_H_ */

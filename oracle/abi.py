@@ -59,6 +59,12 @@ class RcSynthSpec(C.Structure):
                 ("seed", C.c_uint64)]
 
 
+class RcScattering(C.Structure):
+    _fields_ = [("nB", C.c_int), ("nQ", C.c_int), ("nA", C.c_int),
+                ("ksca", C.POINTER(C.c_float)), ("kabs", C.POINTER(C.c_float)),
+                ("theta", C.POINTER(C.c_float)), ("phase_cdf", C.POINTER(C.c_float))]
+
+
 class RcBundleId(C.Structure):
     _fields_ = [("kind", C.c_int), ("i", C.c_int), ("j", C.c_int), ("k", C.c_int), ("v", C.c_int),
                 ("h", C.c_int)]

@@ -28,6 +28,7 @@ namespace {
 template <typename R> struct M;
 template <> struct M<float> {
     static float expm1_(float x) { return rc_expm1f(x); }
+    static float log_(float x) { return rc_logf(x); }
     static float sqrt_(float x) { return sqrtf(x); }
     static void sincos2pi_(float u, float *s, float *c) { rc_sincos2pif(u, s, c); }
     static float fma_(float a, float b, float c) { return fmaf(a, b, c); }
@@ -35,6 +36,7 @@ template <> struct M<float> {
 };
 template <> struct M<double> {
     static double expm1_(double x) { return rc_expm1(x); }
+    static double log_(double x) { return rc_log(x); }
     static double sqrt_(double x) { return sqrt(x); }
     static void sincos2pi_(double u, double *s, double *c) { rc_sincos2pi(u, s, c); }
     static double fma_(double a, double b, double c) { return fma(a, b, c); }
@@ -147,6 +149,20 @@ int find_idx(const R *cdf, int n, R u) {
 // parity tests can measure what the defect does to the wall fluxes.
 int g_ref_wall_edge = 0;
 
+// Particle scattering tables of later solves (oracle_set_scattering), raw
+// as the caller gave them: no scattering while nA == 0.  The march
+// restates the device's scattering step (rc_device.cuh scatter_start,
+// scatter_turn, march_step with SCAT): free path -ln(u) against the
+// scattering coefficient, polar angle from the band's phase CDF (linear in
+// angle between table angles), uniform azimuth, the standard rotation about
+// the old direction; draws from the bundle's Philox counter with the event
+// number in the fourth word.
+struct ScatTables {
+    int nB = 0, nQ = 0, nA = 0;
+    std::vector<float> ksca, theta, cdf;
+};
+ScatTables g_scat;
+
 template <typename R>
 int find_idx_edge(const R *cdf, int n, R u, R edge0) {
     int lo = 0, w = n;
@@ -180,6 +196,8 @@ struct Problem {
     std::vector<std::vector<std::vector<R>>> Twl;     // per level, per wall
     std::vector<R> Tw0[2];                            // level-0 x-face temperatures [kmax][jmax]
     std::vector<R> kt, Ibt, probg, cdf_f, cdf_s, probq, Ibw, Tnb, kP, wvl, wvr, wvc, prob;
+    int nA = 0;                      // scattering: table angles (0: no scattering)
+    std::vector<R> ksca, pcdf, pth;  // [nB][nQ] scaled, [nB][nA] last = 1, [nA] turns
     oracle_setup su;
     R Tmax, Ibmax_f, Ibmax_w[2], T0, inv_dT;
     int row = 0;
@@ -298,6 +316,19 @@ struct Problem {
         for (int w = 0; w < 6; ++w)
             for (int b = 0; b < nB; ++b)
                 Ibw[(size_t)w * nB + b] = (R)(float)rc_planck((double)p.Tw[w], (double)(float)wvc[b]);
+        nA = 0;
+        if (g_scat.nA > 0) {
+            if (g_scat.nB != nB || g_scat.nQ != nQ) return RC_E_INVALID;
+            nA = g_scat.nA;
+            ksca.resize((size_t)nB * nQ);
+            for (size_t i = 0; i < ksca.size(); ++i) ksca[i] = (R)rc_scatter_coef_scaled(g_scat.ksca[i], p.chanHeight);
+            pcdf.resize((size_t)nB * nA);
+            for (int b = 0; b < nB; ++b)
+                for (int a = 0; a < nA; ++a)
+                    pcdf[(size_t)b * nA + a] = (R)((a == nA - 1) ? 1.0f : g_scat.cdf[(size_t)b * nA + a]);
+            pth.resize(nA);
+            for (int a = 0; a < nA; ++a) pth[a] = (R)rc_angle_turns(g_scat.theta[a]);
+        }
         // scalars: tm, row, kappamax, Ibmax (mc_gpu_noint.cu:74,820-826,1362-1366)
         int tm = (int)((Tmax - Tnb[0]) / (Tnb[1] - Tnb[0]));
         if (tm < 0) {
@@ -405,7 +436,80 @@ struct Problem {
         int ic, jc, kc;
         R xp, yp, zp, sx, sy, sz, isx, isy, isz, tra;
         int flag[3];
+        // scattering: counter words of the bundle, events so far, the
+        // scattering coefficient of its band and g point, optical depth left
+        uint32_t cx, cy, cz;
+        int nev;
+        R ks, tau;
     };
+
+    // Absorption along ds (mc_gpu_noint.cu:358-370).
+    void absorb(Beam &ray, double &De, R ds, R absco, R blackpow, R Ibmax, R ratioI, R invTi4, R tol) const {
+        R em = M<R>::expm1_(-(ds * absco));
+        R alpha = -em;
+        R dI = M<R>::fma_(invTi4, blackpow, (R)-1);
+        R c = Ibmax * ray.tra;
+        c = c * alpha;
+        c = c * ratioI;
+        c = c * dI;
+        De -= (double)c;
+        ray.tra = M<R>::fma_(ray.tra, em, ray.tra);
+        if (ray.tra < tol) {
+            R c2 = (Ibmax * ray.tra) * ratioI;
+            c2 = c2 * dI;
+            De -= (double)c2;
+            ray.tra = 0;
+        }
+    }
+
+    // New direction at the next scattering event of a bundle in band nb and
+    // the optical depth to the event after it.
+    void scatter_turn(Beam &ray, int nb) const {
+        ray.nev += 1;
+        rc_u32x4 c = {ray.cx, ray.cy, ray.cz, (uint32_t)(ray.nev + 1)};
+        rc_u32x4 d = rc_philox4x32_10(c, (uint32_t)p.seed, (uint32_t)(p.seed >> 32));
+        R u_t = (R)rc_u01(d.x), u_p = (R)rc_u01(d.y), u_s = (R)rc_u01(d.z);
+        const R *cdf = &pcdf[(size_t)nb * nA];
+        int lo = 0, hi = nA - 1;
+        while (hi - lo > 1) {
+            int mid = (lo + hi) / 2;
+            if (u_t < cdf[mid]) hi = mid;
+            else lo = mid;
+        }
+        R c0 = cdf[hi - 1], c1 = cdf[hi];
+        R fr = (c1 > c0) ? (u_t - c0) / (c1 - c0) : (R)0;
+        if (fr > (R)1) fr = (R)1;
+        R t0 = pth[hi - 1], t1 = pth[hi];
+        R th = M<R>::fma_(fr, t1 - t0, t0);
+        R st, ct, sp, cp;
+        M<R>::sincos2pi_(th, &st, &ct);
+        M<R>::sincos2pi_(u_p, &sp, &cp);
+        R nx, ny, nz;
+        if (std::fabs(ray.sz) > (R)0.99999) {
+            nx = st * cp;
+            ny = st * sp;
+            nz = (ray.sz > (R)0) ? ct : -ct;
+        } else {
+            R w = M<R>::sqrt_((R)1 - ray.sz * ray.sz);
+            R a = st / w;
+            nx = a * (ray.sx * ray.sz * cp - ray.sy * sp) + ray.sx * ct;
+            ny = a * (ray.sy * ray.sz * cp + ray.sx * sp) + ray.sy * ct;
+            nz = ray.sz * ct - st * cp * w;
+        }
+        if (nx == (R)0) nx = (R)1e-10;
+        if (ny == (R)0) ny = (R)1e-10;
+        if (nz == (R)0) nz = (R)1e-10;
+        ray.sx = nx;
+        ray.sy = ny;
+        ray.sz = nz;
+        ray.isx = (R)1 / nx;
+        ray.isy = (R)1 / ny;
+        ray.isz = (R)1 / nz;
+        ray.flag[0] = ray.sx < 0;
+        ray.flag[1] = ray.sy < 0;
+        ray.flag[2] = ray.sz < 0;
+        ray.tau = -M<R>::log_(u_s);
+    }
 
     R Tcell(int lev, int ic, int jc, int kc) const {
         const Grid &G = grid[lev];
@@ -497,27 +601,29 @@ struct Problem {
             R ds = dsx;
             if (ds > dsy) ds = dsy;
             if (ds > dsz) ds = dsz;
+            if (nA > 0) {
+                R dts = ds * ray.ks;
+                if (dts > ray.tau) {
+                    // the next scattering event lies inside this cell
+                    R dsc = ray.tau / ray.ks;
+                    if (dsc > ds) dsc = ds;
+                    ray.xp = M<R>::fma_(dsc, ray.sx, ray.xp);
+                    ray.yp = M<R>::fma_(dsc, ray.sy, ray.yp);
+                    ray.zp = M<R>::fma_(dsc, ray.sz, ray.zp);
+                    absorb(ray, De, dsc, absco, blackpow, Ibmax, ratioI, invTi4, tol);
+                    scatter_turn(ray, nb);
+                    counter += 1;
+                    continue;
+                }
+                ray.tau = ray.tau - dts;
+            }
             if (ds == dsx) ray.xp = fxu;
             else ray.xp = M<R>::fma_(ds, ray.sx, ray.xp);
             if (ds == dsy) ray.yp = fyu;
             else ray.yp = M<R>::fma_(ds, ray.sy, ray.yp);
             if (ds == dsz) ray.zp = fzu;
             else ray.zp = M<R>::fma_(ds, ray.sz, ray.zp);
-            R em = M<R>::expm1_(-(ds * absco));
-            R alpha = -em;
-            R dI = M<R>::fma_(invTi4, blackpow, (R)-1);
-            R c = Ibmax * ray.tra;
-            c = c * alpha;
-            c = c * ratioI;
-            c = c * dI;
-            De -= (double)c;
-            ray.tra = M<R>::fma_(ray.tra, em, ray.tra);
-            if (ray.tra < tol) {
-                R c2 = (Ibmax * ray.tra) * ratioI;
-                c2 = c2 * dI;
-                De -= (double)c2;
-                ray.tra = 0;
-            }
+            absorb(ray, De, ds, absco, blackpow, Ibmax, ratioI, invTi4, tol);
             int axis;
             if (dsx < dsy) axis = (dsx < dsz) ? 0 : 2;
             else axis = (dsy < dsz) ? 1 : 2;
@@ -618,6 +724,20 @@ struct Problem {
         ray.isx = (R)1 / ray.sx;
         ray.isy = (R)1 / ray.sy;
         ray.isz = (R)1 / ray.sz;
+        // scattering: the bundle's counter words, its coefficient and the
+        // optical depth to its first event (draw 1)
+        ray.cx = ctr.x;
+        ray.cy = ctr.y;
+        ray.cz = ctr.z;
+        ray.nev = 0;
+        ray.ks = 0;
+        ray.tau = (R)3.0e38f;
+        if (nA > 0) {
+            rc_u32x4 c1 = {ctr.x, ctr.y, ctr.z, 1u};
+            rc_u32x4 d1 = rc_philox4x32_10(c1, (uint32_t)p.seed, (uint32_t)(p.seed >> 32));
+            ray.tau = -M<R>::log_((R)rc_u01(d1.x));
+            ray.ks = ksca[(size_t)nb * nQ + g];
+        }
         if (rec) {
             rec->nb = nb;
             rec->g = g;
@@ -917,7 +1037,7 @@ int oracle_level_T(const rc_params *p, const float *T, int level, float *out) {
 }  // extern "C"
 
 // Exposes the shared arithmetic primitives to the tests (Philox and the
-// exp/expm1/sincos/Planck functions of radchan_math.h).
+// exp/expm1/sincos/Planck/log functions of radchan_math.h).
 extern "C" int oracle_math_probe(int which, int n, const double *in, double *out) {
     for (int i = 0; i < n; ++i) {
         const double x = in[i];
@@ -929,6 +1049,8 @@ extern "C" int oracle_math_probe(int which, int n, const double *in, double *out
             case 4: { float s, c; rc_sincos2pif((float)x, &s, &c); out[2 * i] = s; out[2 * i + 1] = c; break; }
             case 5: { double s, c; rc_sincos2pi(x, &s, &c); out[2 * i] = s; out[2 * i + 1] = c; break; }
             case 6: out[i] = rc_planck(x, in[n + i]); break;
+            case 7: out[i] = (double)rc_logf((float)x); break;
+            case 8: out[i] = rc_log(x); break;
             default: return RC_E_INVALID;
         }
     }
@@ -991,6 +1113,22 @@ void gl_rule(int n, std::vector<double> &x, std::vector<double> &w) {
     }
 }
 }  // namespace
+
+// Scattering tables for the oracle's later solves and traces (NULL: none).
+// The same checks as the library's rc_scattering_validate are left to the
+// callers (tests); dimensions must match the solve's bands and g points.
+extern "C" int oracle_set_scattering(const rc_scattering *s) {
+    g_scat = ScatTables();
+    if (!s) return 0;
+    if (s->nB < 1 || s->nQ < 1 || s->nA < 2 || !s->ksca || !s->theta || !s->phase_cdf) return RC_E_INVALID;
+    g_scat.nB = s->nB;
+    g_scat.nQ = s->nQ;
+    g_scat.nA = s->nA;
+    g_scat.ksca.assign(s->ksca, s->ksca + (size_t)s->nB * s->nQ);
+    g_scat.theta.assign(s->theta, s->theta + s->nA);
+    g_scat.cdf.assign(s->phase_cdf, s->phase_cdf + (size_t)s->nB * s->nA);
+    return 0;
+}
 
 extern "C" int oracle_set_ref_wall_edge(int on) {
     g_ref_wall_edge = on ? 1 : 0;

@@ -38,6 +38,9 @@ int oracle_setup_scalars(const rc_params *p, const rc_tables *t, const float *T,
 int oracle_grid_level(const rc_params *p, int level, float *xu, float *yu, float *zu, float *x, float *y, float *z);
 /* cell temperatures of a multigrid level, [km][jm][im] */
 int oracle_level_T(const rc_params *p, const float *T, int level, float *out);
+/* particle scattering of later solves and traces (NULL: none); the arrays
+ * are copied */
+int oracle_set_scattering(const rc_scattering *s);
 
 #ifdef __cplusplus
 }

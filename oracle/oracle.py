@@ -69,7 +69,51 @@ def _pp(p):
     return C.byref(L.params(p))
 
 
-def solve(p, tables, T, zstart=1, rpt=8, cell_begin=0, cell_end=-1, walls=True, fp64=False, nthreads=0):
+class _Scattering:
+    """Holds the arrays of particle scattering tables while the oracle
+    solves with them: ksca [nB, nQ], theta [nA] (radians), phase_cdf
+    [nB, nA]."""
+
+    def __init__(self, ksca, theta, phase_cdf):
+        self.k = np.ascontiguousarray(ksca, np.float32)
+        self.t = np.ascontiguousarray(theta, np.float32)
+        self.c = np.ascontiguousarray(phase_cdf, np.float32)
+        nB, nQ = self.k.shape
+        self.s = L.RcScattering(nB, nQ, self.t.shape[0], _fp(self.k), None, _fp(self.t), _fp(self.c))
+
+
+class scattering:
+    """Context manager: the oracle's solves and traces inside it see the
+    given particle scattering tables (an object with ksca, theta, phase_cdf
+    arrays, or a dict with those keys); None means none."""
+
+    def __init__(self, sc):
+        self.sc = sc
+
+    def __enter__(self):
+        if self.sc is not None:
+            g = (lambda k: self.sc[k]) if isinstance(self.sc, dict) else (lambda k: getattr(self.sc, k))
+            self.h = _Scattering(g("ksca"), g("theta"), g("phase_cdf"))
+            f = lib().oracle_set_scattering
+            f.restype = C.c_int
+            f.argtypes = [C.POINTER(L.RcScattering)]
+            if f(C.byref(self.h.s)) != 0:
+                raise RuntimeError("oracle_set_scattering failed")
+        return self
+
+    def __exit__(self, *a):
+        f = lib().oracle_set_scattering
+        f.restype = C.c_int
+        f.argtypes = [C.POINTER(L.RcScattering)]
+        f(None)
+        return False
+
+
+def solve(p, tables, T, zstart=1, rpt=8, cell_begin=0, cell_end=-1, walls=True, fp64=False, nthreads=0,
+          scatter=None):
+    if scatter is not None:
+        with scattering(scatter):
+            return solve(p, tables, T, zstart, rpt, cell_begin, cell_end, walls, fp64, nthreads)
     T = np.ascontiguousarray(T, dtype=np.float32)
     kl = p.kmax // p.p_col
     q = np.full((kl, p.jmax, p.imax), np.nan)
@@ -85,7 +129,10 @@ def solve(p, tables, T, zstart=1, rpt=8, cell_begin=0, cell_end=-1, walls=True, 
     return dict(q64=q, var64=v, qw64=qw, vw64=vw, steps=st.value, bundles=nb.value)
 
 
-def trace(p, tables, T, ids, max_cells=0, fp64=False):
+def trace(p, tables, T, ids, max_cells=0, fp64=False, scatter=None):
+    if scatter is not None:
+        with scattering(scatter):
+            return trace(p, tables, T, ids, max_cells, fp64)
     T = np.ascontiguousarray(T, dtype=np.float32)
     n = len(ids)
     arr = (L.RcBundleId * n)(*[L.RcBundleId(*b) for b in ids])

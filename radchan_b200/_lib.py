@@ -65,6 +65,18 @@ class RcSynthSpec(C.Structure):
                 ("seed", C.c_uint64)]
 
 
+class RcScattering(C.Structure):
+    _fields_ = [("nB", C.c_int), ("nQ", C.c_int), ("nA", C.c_int),
+                ("ksca", _FP), ("kabs", _FP), ("theta", _FP), ("phase_cdf", _FP)]
+
+
+class RcScatterSpec(C.Structure):
+    _fields_ = [("nB", C.c_int), ("nQ", C.c_int), ("nA", C.c_int),
+                ("ksca_lo", C.c_double), ("ksca_hi", C.c_double),
+                ("g_lo", C.c_double), ("g_hi", C.c_double),
+                ("seed", C.c_uint64)]
+
+
 class RcBundleId(C.Structure):
     _fields_ = [("kind", C.c_int), ("i", C.c_int), ("j", C.c_int), ("k", C.c_int), ("v", C.c_int),
                 ("h", C.c_int)]
@@ -114,8 +126,15 @@ _SIGS = [
     ("rc_tables_view", _I, [_VP, C.POINTER(RcTables)]),
     ("rc_tables_validate", _I, [C.POINTER(RcTables), C.c_char_p, C.c_size_t]),
     ("rc_tables_free", None, [_VP]),
+    ("rc_scattering_synthetic", _I, [C.POINTER(RcScatterSpec), C.POINTER(_VP)]),
+    ("rc_scattering_read_dir", _I, [C.c_char_p, _I, _I, C.POINTER(_VP)]),
+    ("rc_scattering_write_dir", _I, [_VP, C.c_char_p]),
+    ("rc_scattering_validate", _I, [C.POINTER(RcScattering), C.c_char_p, C.c_size_t]),
+    ("rc_scattering_view", _I, [_VP, C.POINTER(RcScattering)]),
+    ("rc_scattering_free", None, [_VP]),
     ("rc_create", _I, [C.POINTER(RcParams), _I, C.POINTER(_VP)]),
     ("rc_set_tables", _I, [_VP, C.POINTER(RcTables)]),
+    ("rc_set_scattering", _I, [_VP, C.POINTER(RcScattering)]),
     ("rc_solve_async", _I, [_VP, _FP, _I, C.POINTER(C.c_int32)]),
     ("rc_solve_device_async", _I, [_VP, _VP, _I, C.POINTER(C.c_int32)]),
     ("rc_collect", _I, [_VP, C.c_int32, _FP, _FP, _DP, _DP, _DP, _DP]),

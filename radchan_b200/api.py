@@ -111,6 +111,75 @@ class TableSet:
             pass
 
 
+class Scattering:
+    """Particle scattering tables (rc_scattering): scattering coefficient per
+    band and g point, phase-function CDF per band over nA angles.  Either
+    host-owned by the library (synthetic, read_dir) or built from numpy
+    arrays (from_arrays)."""
+
+    def __init__(self, handle=None, arrays=None):
+        self.h = None
+        self._keep = None
+        if handle is not None:
+            self.h = C.c_void_p(handle) if not isinstance(handle, C.c_void_p) else handle
+            self.view = L.RcScattering()
+            L.check(L.lib().rc_scattering_view(self.h, C.byref(self.view)))
+        else:
+            ksca, theta, cdf, kabs = arrays
+            self._keep = [np.ascontiguousarray(a, np.float32) for a in (ksca, theta, cdf)]
+            self._keep.append(None if kabs is None else np.ascontiguousarray(kabs, np.float32))
+            k, th, cd, ka = self._keep
+            fp = lambda a: a.ctypes.data_as(C.POINTER(C.c_float)) if a is not None else None
+            self.view = L.RcScattering(k.shape[0], k.shape[1], th.shape[0], fp(k), fp(ka), fp(th), fp(cd))
+
+    @classmethod
+    def from_arrays(cls, ksca, theta, phase_cdf, kabs=None):
+        """ksca [nB, nQ] (1/m), theta [nA] radians, phase_cdf [nB, nA]."""
+        ksca = np.asarray(ksca, np.float32)
+        phase_cdf = np.asarray(phase_cdf, np.float32)
+        assert ksca.ndim == 2 and phase_cdf.ndim == 2 and phase_cdf.shape[0] == ksca.shape[0]
+        assert phase_cdf.shape[1] == len(theta)
+        return cls(arrays=(ksca, theta, phase_cdf, kabs))
+
+    @classmethod
+    def synthetic(cls, nB, nQ=1, nA=181, ksca_lo=0.5, ksca_hi=0.5, g_lo=0.0, g_hi=0.0, seed=77):
+        s = L.RcScatterSpec(nB, nQ, nA, ksca_lo, ksca_hi, g_lo, g_hi, seed)
+        h = C.c_void_p()
+        L.check(L.lib().rc_scattering_synthetic(C.byref(s), C.byref(h)))
+        return cls(handle=h)
+
+    @classmethod
+    def read_dir(cls, path, nB, nQ):
+        h = C.c_void_p()
+        L.check(L.lib().rc_scattering_read_dir(str(path).encode(), nB, nQ, C.byref(h)))
+        return cls(handle=h)
+
+    def write_dir(self, path):
+        assert self.h is not None, "only library-owned particle tables are written"
+        L.check(L.lib().rc_scattering_write_dir(self.h, str(path).encode()))
+
+    def validate(self) -> str:
+        buf = C.create_string_buffer(512)
+        rc = L.lib().rc_scattering_validate(C.byref(self.view), buf, 512)
+        return "" if rc == L.RC_OK else buf.value.decode(errors="replace")
+
+    def arrays(self):
+        v = self.view
+        nB, nQ, nA = v.nB, v.nQ, v.nA
+        f = lambda ptr, n: np.ctypeslib.as_array(ptr, shape=(n,)).copy()
+        return dict(nB=nB, nQ=nQ, nA=nA, ksca=f(v.ksca, nB * nQ).reshape(nB, nQ),
+                    kabs=f(v.kabs, nB * nQ).reshape(nB, nQ) if v.kabs else None, theta=f(v.theta, nA),
+                    phase_cdf=f(v.phase_cdf, nB * nA).reshape(nB, nA))
+
+    def __del__(self):
+        try:
+            if self.h:
+                L.lib().rc_scattering_free(self.h)
+                self.h = None
+        except Exception:
+            pass
+
+
 def rel_std_maxq(q, sigma):
     """Relative Monte Carlo standard deviation of max|Q|: RMS sigma of the
     cells whose |Q| is within 10% of the maximum, over max|Q| (the
@@ -239,6 +308,12 @@ class Solver:
 
     def set_launch(self, rays_per_thread=0, block_threads=0, sort_bands=-1, occupancy=0):
         L.check(L.lib().rc_set_launch(self.ctx, rays_per_thread, block_threads, sort_bands, occupancy), self.ctx)
+
+    def set_scattering(self, sc: "Scattering | None"):
+        """rc_set_scattering: particle scattering for later solves (None
+        removes it)."""
+        self.scattering = sc
+        L.check(L.lib().rc_set_scattering(self.ctx, C.byref(sc.view) if sc is not None else None), self.ctx)
 
     def set_priority(self, threshold: float):
         """rc_set_priority: tiles holding a bundle with |s_x| < threshold

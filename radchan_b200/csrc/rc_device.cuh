@@ -113,6 +113,12 @@ struct DSolve {
     const R *ibm;             // [nB] I_b(Tmax) (wall OERM weight denominator)
     const int *guide_f;       // [kGuide] first band with cdf_f > q/kGuide
     const int *guide_s;       // [kGuide] same for cdf_s
+    // scattering particles (nA = 0: none)
+    const R *ksca;            // [nB][nQ] scattering coefficient (scaled by chanHeight)
+    const R *pcdf;            // [nB][nA] cumulative phase-function probability, last = 1
+    const R *pth;             // [nA] scattering angles in turns (theta / 2 pi)
+    int nA;
+    int pad3;
     DScalars *sc;
     double *partial;
     long long n_fluid_items, n_items, n_tiles;
@@ -137,7 +143,7 @@ struct DSolve {
 enum RcSite : int {
     SITE_FACE = 1, SITE_PYRAMID, SITE_ROW, SITE_IBW, SITE_WALL_T, SITE_WALL_ROW, SITE_CENTRE, SITE_EMIT_T,
     SITE_WALL_EMIT_T, SITE_FACE_SHIFT, SITE_EMIT_ROW, SITE_DEN, SITE_IBM, SITE_PROBG, SITE_PARTIAL, SITE_LEVEL,
-    SITE_CDF
+    SITE_CDF, SITE_KSCA, SITE_PHASE
 };
 #if RC_CHECKED
 __device__ __forceinline__ long long rc_ix(long long i, long long n, int site, DScalars *sc) {
@@ -157,6 +163,7 @@ __device__ __forceinline__ long long rc_ix(long long i, long long n, int site, D
 template <typename R> struct RT;
 template <> struct RT<float> {
     static __device__ __forceinline__ float expm1_(float x) { return rc_expm1f(x); }
+    static __device__ __forceinline__ float log_(float x) { return rc_logf(x); }
     static __device__ __forceinline__ float sqrt_(float x) { return sqrtf(x); }
     static __device__ __forceinline__ float fma_(float a, float b, float c) { return fmaf(a, b, c); }
     static __device__ __forceinline__ float lerp_(float a0, float a1, float w) { return rc_lerpf(a0, a1, w); }
@@ -167,6 +174,7 @@ template <> struct RT<float> {
 };
 template <> struct RT<double> {
     static __device__ __forceinline__ double expm1_(double x) { return rc_expm1(x); }
+    static __device__ __forceinline__ double log_(double x) { return rc_log(x); }
     static __device__ __forceinline__ double sqrt_(double x) { return sqrt(x); }
     static __device__ __forceinline__ double fma_(double a, double b, double c) { return fma(a, b, c); }
     static __device__ __forceinline__ double lerp_(double a0, double a1, double w) { return rc_lerp(a0, a1, w); }
@@ -490,13 +498,172 @@ __device__ __forceinline__ void hit_wall(Ray<R> &r, const DSolve<R> &S, const DL
     }
 }
 
+// Absorption along a path of length ds in a cell of absorption coefficient
+// absco and blackbody intensity blackpow: the step's OERM tally, the
+// transmissivity update and the cutoff deposit (:358-370).
+template <typename R>
+__device__ __forceinline__ void absorb(Ray<R> &r, R ds, R absco, R blackpow) {
+    const R em = RT<R>::expm1_(-(ds * absco));
+    const R alpha = -em;
+    const R dI = RT<R>::fma_(r.invTi4, blackpow, (R)-1);
+    R c = r.Ibmax * r.tra;
+    c = c * alpha;
+    c = c * r.ratioI;
+    c = c * dI;
+    r.De -= (double)c;
+    r.tra = RT<R>::fma_(r.tra, em, r.tra);
+    if (r.tra < r.tol) {  // cutoff: deposit the rest here (:365-370)
+        R c2 = (r.Ibmax * r.tra) * r.ratioI;
+        c2 = c2 * dI;
+        r.De -= (double)c2;
+        r.tra = (R)0;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// scattering by suspended particles
+// ---------------------------------------------------------------------------
+// The reference's Monte Carlo path has no scattering; nbcorrk tabulates the
+// particles' scattering coefficient per band and g point and their phase
+// function per band (nbcorrk/write_tables.cpp:204-260, :326-336).  A bundle
+// of a scattering medium carries, besides its Ray, the Philox counter words
+// of its emission (h, v | kind << 24, cell): draw n (the fourth counter word
+// n >= 1; emission uses 0) is its n-th draw after emission.  Draw 1 gives
+// the optical depth to the first scattering event, tau = -ln(u); at event n
+// draw n+1 gives the scattering angle (the band's cumulative phase
+// probability inverted, linear in angle between table angles), the azimuth
+// (uniform) and the optical depth to the next event.  The free path is
+// sampled against the scattering coefficient alone; absorption stays the
+// continuous OERM tally, so the emission-based reciprocity weights are
+// unchanged (the exchange between two cells is reciprocal for a phase
+// function of the scattering angle alone).
+template <typename R>
+struct ScatState {
+    uint32_t cx, cy, cz;  // Philox counter words of the bundle
+    int nev;              // scattering events so far
+    R ks;                 // scattering coefficient of the bundle's band and g point
+    R tau;                // optical depth left to the next event
+};
+
+// A ring entry of a scattering medium: the emitted bundle, its counter
+// words and the optical depth to its first event.
+template <typename R>
+struct alignas(16) EmittedScat {
+    Emitted<R> e;
+    uint32_t cx, cy, cz;
+    R tau;
+};
+
+// The counter words and first free path of an emitted bundle (draw 1).
+template <typename R>
+__device__ __forceinline__ void scatter_start(uint32_t &cx, uint32_t &cy, uint32_t &cz, R &tau, const DSolve<R> &S,
+                                              int kind, int i, int j, int k, int v, int h) {
+    cx = (uint32_t)h;
+    cy = (uint32_t)v | ((uint32_t)kind << 24);
+    cz = (kind == 0) ? (uint32_t)((i - 1) + S.imax * ((j - 1) + S.jmax * (k - 1)))
+                     : (uint32_t)((j - 1) + S.jmax * (k - 1));
+    if (S.nA > 0) {
+        rc_u32x4 c;
+        c.x = cx;
+        c.y = cy;
+        c.z = cz;
+        c.w = 1u;
+        const rc_u32x4 d = rc_philox4x32_10(c, S.key0, S.key1);
+        tau = -RT<R>::log_((R)rc_u01(d.x));
+    } else {
+        tau = (R)3.0e38f;
+    }
+}
+
+// New direction at scattering event q.nev + 1 of a bundle in band nb, and
+// the optical depth to the event after it.  The direction is turned by the
+// sampled polar angle theta about the old one, with azimuth phi measured
+// from the plane of the old direction and the z axis (the standard rotation
+// of Monte Carlo transport codes; near |s_z| = 1 the new direction is taken
+// about the z axis itself).  Zero components are floored to 1e-10 as at
+// emission (:132-137).
+template <typename R>
+__device__ __noinline__ void scatter_turn(Ray<R> &r, ScatState<R> &q, const DSolve<R> &S) {
+    q.nev += 1;
+    rc_u32x4 c;
+    c.x = q.cx;
+    c.y = q.cy;
+    c.z = q.cz;
+    c.w = (uint32_t)(q.nev + 1);
+    const rc_u32x4 d = rc_philox4x32_10(c, S.key0, S.key1);
+    const R u_t = (R)rc_u01(d.x), u_p = (R)rc_u01(d.y), u_s = (R)rc_u01(d.z);
+    const int nA = S.nA;
+    const R *cdf = S.pcdf + RC_IX((size_t)r.nb * nA, (long long)S.nB * nA, SITE_PHASE, S);
+    int lo = 0, hi = nA - 1;
+    while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (u_t < cdf[mid]) hi = mid;
+        else lo = mid;
+    }
+    const R c0 = cdf[hi - 1], c1 = cdf[hi];
+    R fr = (c1 > c0) ? (u_t - c0) / (c1 - c0) : (R)0;
+    if (fr > (R)1) fr = (R)1;
+    const R t0 = S.pth[hi - 1], t1 = S.pth[hi];
+    const R th = RT<R>::fma_(fr, t1 - t0, t0);
+    R st, ct, sp, cp;
+    RT<R>::sincos2pi_(th, &st, &ct);
+    RT<R>::sincos2pi_(u_p, &sp, &cp);
+    R nx, ny, nz;
+    if (RT<R>::fabs_(r.sz) > (R)0.99999) {
+        nx = st * cp;
+        ny = st * sp;
+        nz = (r.sz > (R)0) ? ct : -ct;
+    } else {
+        const R w = RT<R>::sqrt_((R)1 - r.sz * r.sz);
+        const R a = st / w;
+        nx = a * (r.sx * r.sz * cp - r.sy * sp) + r.sx * ct;
+        ny = a * (r.sy * r.sz * cp + r.sx * sp) + r.sy * ct;
+        nz = r.sz * ct - st * cp * w;
+    }
+    if (nx == (R)0) nx = (R)1e-10;
+    if (ny == (R)0) ny = (R)1e-10;
+    if (nz == (R)0) nz = (R)1e-10;
+    r.sx = nx;
+    r.sy = ny;
+    r.sz = nz;
+    r.isx = (R)1 / nx;
+    r.isy = (R)1 / ny;
+    r.isz = (R)1 / nz;
+    q.tau = -RT<R>::log_(u_s);
+}
+
+// Scattering state of a bundle taken from the ring.
+template <typename R>
+__device__ __forceinline__ void place_scatter(ScatState<R> &q, const DSolve<R> &S, const EmittedScat<R> &e) {
+    q.cx = e.cx;
+    q.cy = e.cy;
+    q.cz = e.cz;
+    q.tau = e.tau;
+    q.nev = 0;
+    const int nb = e.e.nbg & 0xfffff, g = e.e.nbg >> 20;
+    q.ks = (S.nA > 0) ? S.ksca[RC_IX((size_t)nb * S.nQ + g, (long long)S.nB * S.nQ, SITE_KSCA, S)] : (R)0;
+}
+
+// The emitted bundle inside a ring entry of either kind.
+template <typename R>
+__device__ __forceinline__ Emitted<R> &entry_base(Emitted<R> &e) { return e; }
+template <typename R>
+__device__ __forceinline__ Emitted<R> &entry_base(EmittedScat<R> &e) { return e.e; }
+template <typename R>
+__device__ __forceinline__ const Emitted<R> &entry_base(const Emitted<R> &e) { return e; }
+template <typename R>
+__device__ __forceinline__ const Emitted<R> &entry_base(const EmittedScat<R> &e) { return e.e; }
+
 // One ray-cell crossing (one iteration of the while loop of march_ray,
 // :252-656).  Returns the step budget (maxs) of the level the step was
 // taken on, which the caller compares with the step counter.  The side of
 // the cell a ray leaves through on each axis follows from the sign of its
-// direction component (never 0: emission floors it at 1e-10).
-template <typename R>
-__device__ __forceinline__ int march_step(Ray<R> &r, const DSolve<R> &S) {
+// direction component (never 0: emission floors it at 1e-10).  With SCAT, a
+// bundle whose scattering optical depth over the step exceeds what is left
+// to its next event stops at the event inside the cell (absorbing along
+// the shortened path), turns, and counts the event as a step.
+template <typename R, bool SCAT>
+__device__ __forceinline__ int march_step(Ray<R> &r, ScatState<R> &qs, const DSolve<R> &S) {
     // S lives in global memory (read-only during every kernel that steps)
     const int4 A = __ldg(&S.lva[RC_IX(r.lev, S.nlev, SITE_LEVEL, S)]);
     const int4 B = __ldg(&S.lvb[RC_IX(r.lev, S.nlev, SITE_LEVEL, S)]);
@@ -519,24 +686,26 @@ __device__ __forceinline__ int march_step(Ray<R> &r, const DSolve<R> &S) {
     R ds = dsx;
     if (ds > dsy) ds = dsy;
     if (ds > dsz) ds = dsz;
+    if constexpr (SCAT) {
+        const R dts = ds * qs.ks;
+        if (dts > qs.tau) {
+            // the next scattering event lies inside this cell
+            R dsc = qs.tau / qs.ks;
+            if (dsc > ds) dsc = ds;
+            r.xp = RT<R>::fma_(dsc, r.sx, r.xp);
+            r.yp = RT<R>::fma_(dsc, r.sy, r.yp);
+            r.zp = RT<R>::fma_(dsc, r.sz, r.zp);
+            absorb(r, dsc, absco, blackpow);
+            scatter_turn(r, qs, S);
+            r.counter += 1;
+            return B.w;
+        }
+        qs.tau = qs.tau - dts;
+    }
     r.xp = (ds == dsx) ? fxu : RT<R>::fma_(ds, r.sx, r.xp);
     r.yp = (ds == dsy) ? fyu : RT<R>::fma_(ds, r.sy, r.yp);
     r.zp = (ds == dsz) ? fzu : RT<R>::fma_(ds, r.sz, r.zp);
-    const R em = RT<R>::expm1_(-(ds * absco));
-    const R alpha = -em;
-    const R dI = RT<R>::fma_(r.invTi4, blackpow, (R)-1);
-    R c = r.Ibmax * r.tra;
-    c = c * alpha;
-    c = c * r.ratioI;
-    c = c * dI;
-    r.De -= (double)c;
-    r.tra = RT<R>::fma_(r.tra, em, r.tra);
-    if (r.tra < r.tol) {  // cutoff: deposit the rest here (:365-370)
-        R c2 = (r.Ibmax * r.tra) * r.ratioI;
-        c2 = c2 * dI;
-        r.De -= (double)c2;
-        r.tra = (R)0;
-    }
+    absorb(r, ds, absco, blackpow);
     // crossed axis (ties: x only if strictly smallest, :375-377, 524)
     const int axis = (dsx < dsy) ? ((dsx < dsz) ? 0 : 2) : ((dsy < dsz) ? 1 : 2);
     const bool ax0 = axis == 0, ax1 = axis == 1;

@@ -54,6 +54,22 @@ int tables_write_dir(const TableSet &ts, const std::string &dir, std::string &er
 // naming the first violation otherwise.
 int tables_check(const TableSet &t, std::string &err);
 
+// Host copy of a particle scattering table set (rc_scattering layouts).
+struct ScatterSet {
+    int nB = 0, nQ = 0, nA = 0;
+    std::vector<float> wvl, wvr, wvc;   // [nB] band edges and centres (0 when synthetic)
+    std::vector<float> kabs, ksca;      // [nB][nQ]
+    std::vector<float> theta;           // [nA] radians
+    std::vector<float> cdf;             // [nB][nA]
+    void view(rc_scattering *s) const;
+};
+
+int scattering_synthetic(const rc_scatter_spec &spec, ScatterSet &out, std::string &err);
+int scattering_read_dir(const std::string &dir, int nB, int nQ, ScatterSet &out, std::string &err);
+int scattering_write_dir(const ScatterSet &s, const std::string &dir, std::string &err);
+// The checks of rc_scattering_validate.
+int scattering_check(const rc_scattering &s, std::string &err);
+
 // Gauss-Legendre nodes/weights on [-1, 1] (Newton iteration on P_n).
 void gauss_legendre(int n, std::vector<double> &x, std::vector<double> &w);
 
@@ -67,7 +83,10 @@ double synth_uniform(uint64_t seed, uint32_t stream, uint32_t idx);
 
 }  // namespace rc
 
-// Opaque handle of the C ABI.
+// Opaque handles of the C ABI.
 struct rc_table_set {
     rc::TableSet ts;
+};
+struct rc_scatter_set {
+    rc::ScatterSet s;
 };

@@ -242,6 +242,9 @@ struct Impl : ImplBase {
     R *d_Ibw = nullptr, *d_Tnb = nullptr, *d_kP = nullptr, *d_wvl = nullptr, *d_wvr = nullptr, *d_wvc = nullptr;
     KIRow<R> *d_ki = nullptr;
     int nT = 0, nB = 0, nQ = 0;
+    // scattering particles (rc_set_scattering): coefficient, phase CDF, angles in turns
+    R *d_ksca = nullptr, *d_pcdf = nullptr, *d_pth = nullptr;
+    int nA = 0;
     std::vector<Slot<R>> slots;
     int smem_opt_in = 0;
 
@@ -271,6 +274,14 @@ struct Impl : ImplBase {
         dfree(d_wvr);
         dfree(d_wvc);
         dfree(d_ki);
+        release_scattering();
+    }
+
+    void release_scattering() {
+        dfree(d_ksca);
+        dfree(d_pcdf);
+        dfree(d_pth);
+        nA = 0;
     }
 
     void release() {
@@ -487,9 +498,12 @@ struct Impl : ImplBase {
         RC_CK(cudaGetDeviceProperties(&prop, c->device));
         c->num_sms = prop.multiProcessorCount;
         smem_opt_in = (int)prop.sharedMemPerBlockOptin;
-        RC_CK(cudaFuncSetAttribute(k_march<R, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_opt_in));
-        RC_CK(cudaFuncSetAttribute(k_march<R, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_opt_in));
-        RC_CK(cudaFuncSetAttribute(k_march<R, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_opt_in));
+        RC_CK(cudaFuncSetAttribute(k_march<R, 2, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_opt_in));
+        RC_CK(cudaFuncSetAttribute(k_march<R, 3, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_opt_in));
+        RC_CK(cudaFuncSetAttribute(k_march<R, 4, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_opt_in));
+        RC_CK(cudaFuncSetAttribute(k_march<R, 2, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_opt_in));
+        RC_CK(cudaFuncSetAttribute(k_march<R, 3, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_opt_in));
+        RC_CK(cudaFuncSetAttribute(k_march<R, 4, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_opt_in));
         if (p.grey) return set_grey_tables();
         return RC_OK;
     }
@@ -598,6 +612,47 @@ struct Impl : ImplBase {
         return RC_OK;
     }
 
+    // Scattering particles for later solves (nullptr: none).  The table
+    // must match the context's bands and g points (grey: grey_nB bands, one
+    // g point).  ksca is scaled by chanHeight like k (read_tables.cpp:30,56);
+    // angles become turns (theta / 2 pi), the argument of the march's
+    // sin/cos; the last CDF entry of every band is set to exactly 1.
+    int set_scattering(const rc_scattering *s) {
+        std::string *err_ = &c->err;
+        const rc_params &p = c->p;
+        if (!s) {
+            RC_CK(cudaDeviceSynchronize());
+            release_scattering();
+            return RC_OK;
+        }
+        const int nBc = p.grey ? p.grey_nB : p.nB, nQc = p.grey ? 1 : p.nQ;
+        if (s->nB != nBc || s->nQ != nQc)
+            return set_err(err_, RC_E_INVALID, "scattering table bands / g points differ from the context's");
+        {
+            char msg[256];
+            if (rc_scattering_validate(s, msg, sizeof(msg))) return set_err(err_, RC_E_INVALID, msg);
+        }
+        // a kernel still reading the old arrays (a solve or batch of this
+        // context) finishes before they are freed
+        RC_CK(cudaDeviceSynchronize());
+        std::vector<float> ks((size_t)s->nB * s->nQ), cdf((size_t)s->nB * s->nA), th(s->nA);
+        for (size_t i = 0; i < ks.size(); ++i) ks[i] = rc_scatter_coef_scaled(s->ksca[i], p.chanHeight);
+        for (int b = 0; b < s->nB; ++b)
+            for (int a = 0; a < s->nA; ++a)
+                cdf[(size_t)b * s->nA + a] = (a == s->nA - 1) ? 1.0f : s->phase_cdf[(size_t)b * s->nA + a];
+        for (int a = 0; a < s->nA; ++a) th[a] = rc_angle_turns(s->theta[a]);
+        release_scattering();
+        int rc = upload(d_ksca, ks, err_);
+        if (!rc) rc = upload(d_pcdf, cdf, err_);
+        if (!rc) rc = upload(d_pth, th, err_);
+        if (rc) {
+            release_scattering();
+            return rc;
+        }
+        nA = s->nA;
+        return RC_OK;
+    }
+
     // Work decomposition: items of rpt bundles, chunk count padded so that
     // the chunks of one (cell, replicate) never straddle a 32-item tile.
     void decompose(int rpt, int &nchunk, int &gsize, int &nparts) const {
@@ -683,6 +738,10 @@ struct Impl : ImplBase {
         d.ibm = s.d_ibm;
         d.guide_f = s.d_guide_f;
         d.guide_s = s.d_guide_s;
+        d.ksca = d_ksca;
+        d.pcdf = d_pcdf;
+        d.pth = d_pth;
+        d.nA = nA;
         d.probq = d_probq;
         d.Ibw = d_Ibw;
         d.Pw0[0] = s.d_Tw0[0];
@@ -783,10 +842,13 @@ struct Impl : ImplBase {
         return RC_OK;
     }
 
-    size_t march_smem(int block, int rpt_max) const { return march_smem_bytes<R>(block, rpt_max); }
+    size_t march_smem(int block, int rpt_max, bool scat = false) const {
+        return scat ? march_smem_bytes<R, true>(block, rpt_max) : march_smem_bytes<R, false>(block, rpt_max);
+    }
 
-    static void (*march_fn(int minb))(MarchArgs) {
-        return minb <= 2 ? k_march<R, 2> : minb == 3 ? k_march<R, 3> : k_march<R, 4>;
+    static void (*march_fn(int minb, bool scat))(MarchArgs) {
+        if (scat) return minb <= 2 ? k_march<R, 2, true> : minb == 3 ? k_march<R, 3, true> : k_march<R, 4, true>;
+        return minb <= 2 ? k_march<R, 2, false> : minb == 3 ? k_march<R, 3, false> : k_march<R, 4, false>;
     }
 
     // Long-ray priority list of a one-solve launch (k_prio_kmin +
@@ -849,14 +911,17 @@ struct Impl : ImplBase {
         return RC_OK;
     }
 
+    // scat: < 0 takes this context's medium (scattering tables set or not);
+    // a launch over several contexts passes whether any of them scatters.
     int launch_march(const DSolve<R> *d_solves, const long long *d_tiles, int nsolves, long long total_tiles,
                      unsigned long long *d_counter, int block, int rpt_max, cudaStream_t st, int minb = 0,
-                     const Slot<R> *prio = nullptr) {
+                     const Slot<R> *prio = nullptr, int scat = -1) {
         std::string *err_ = &c->err;
         RC_FAILPOINT("march");
         if (minb <= 0) minb = c->minb;
-        auto fn = march_fn(minb);
-        const size_t smem = march_smem(block, rpt_max);
+        const bool sc = scat < 0 ? nA > 0 : scat > 0;
+        auto fn = march_fn(minb, sc);
+        const size_t smem = march_smem(block, rpt_max, sc);
         if ((int)smem > smem_opt_in) return set_err(err_, RC_E_INVALID, "rays_per_thread too large for shared memory");
         int per_sm = 0;
         RC_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, block, smem));
@@ -1058,7 +1123,7 @@ struct Impl : ImplBase {
             for (int bi = 0; bi < 2 && !rc; ++bi)
                 for (int ri = 0; ri < 5 && !rc; ++ri) {
                     const int rpt = rpts[ri], block = blocks[bi], minb = minbs[oi];
-                    if (march_smem(block, rpt) > (size_t)smem_opt_in) continue;
+                    if (march_smem(block, rpt, nA > 0) > (size_t)smem_opt_in) continue;
                     float ms = 0.f;
                     rc = time_config(s, zstart, rpt, block, minb, &ms);
                     if (!rc && ms < best) {
@@ -1238,7 +1303,12 @@ struct Impl : ImplBase {
         if (cells && max_cells > 0) RC_CK(cudaMalloc((void **)&d_cells, (size_t)n * max_cells * 4 * sizeof(int)));
         RC_CK(cudaMemcpy(d_ids, ids, n * sizeof(rc_bundle_id), cudaMemcpyHostToDevice));
         if (d_cells) RC_CK(cudaMemset(d_cells, 0xff, (size_t)n * max_cells * 4 * sizeof(int)));
-        k_trace<R><<<(n + 63) / 64, 64, 0, sp->st>>>(sp->d_desc, n, d_ids, d_out, d_cells ? max_cells : 0, d_cells);
+        if (nA > 0)
+            k_trace<R, true><<<(n + 63) / 64, 64, 0, sp->st>>>(sp->d_desc, n, d_ids, d_out, d_cells ? max_cells : 0,
+                                                               d_cells);
+        else
+            k_trace<R, false><<<(n + 63) / 64, 64, 0, sp->st>>>(sp->d_desc, n, d_ids, d_out, d_cells ? max_cells : 0,
+                                                                d_cells);
         RC_CK(cudaGetLastError());
         RC_CK(cudaStreamSynchronize(sp->st));
         RC_CK(cudaMemcpy(out, d_out, n * sizeof(rc_trace_rec), cudaMemcpyDeviceToHost));

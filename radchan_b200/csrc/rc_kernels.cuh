@@ -298,7 +298,7 @@ __global__ void k_levels(const float *__restrict__ T, int imax, int jmax, int km
 // ---------------------------------------------------------------------------
 // bundle traces: one thread per requested bundle, same device functions
 // ---------------------------------------------------------------------------
-template <typename R>
+template <typename R, bool SCAT>
 __global__ void k_trace(const DSolve<R> *Sp, int n, const rc_bundle_id *ids, rc_trace_rec *out, int max_cells,
                         int *cells) {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
@@ -314,8 +314,10 @@ __global__ void k_trace(const DSolve<R> *Sp, int n, const rc_bundle_id *ids, rc_
     rec.sx = rec.sy = rec.sz = 0.f;
     rec.tra = 0.f;
     rec.De = 0.0;
-    Emitted<R> e;
+    EmittedScat<R> es;
+    Emitted<R> &e = es.e;
     const bool ok = emit_bundle(e, S, id.kind, id.i, id.j, id.k, id.v, id.h);
+    if (SCAT) scatter_start(es.cx, es.cy, es.cz, es.tau, S, id.kind, id.i, id.j, id.k, id.v, id.h);
     rec.nb = e.nbg & 0xfffff;
     rec.g = e.nbg >> 20;
     rec.sx = (float)e.sx;
@@ -323,7 +325,9 @@ __global__ void k_trace(const DSolve<R> *Sp, int n, const rc_bundle_id *ids, rc_
     rec.sz = (float)e.sz;
     if (ok) {
         Ray<R> r;
+        ScatState<R> qs;
         place_bundle(r, S, e);
+        if (SCAT) place_scatter(qs, S, es);
         bool active = level_advance(r, S);
         int ns = 0;
         while (active) {
@@ -334,7 +338,7 @@ __global__ void k_trace(const DSolve<R> *Sp, int n, const rc_bundle_id *ids, rc_
                 c[2] = r.jc;
                 c[3] = r.kc;
             }
-            march_step(r, S);
+            march_step<R, SCAT>(r, qs, S);
             ns++;
             active = r.tra > r.tol;
             if (active) active = level_advance(r, S);

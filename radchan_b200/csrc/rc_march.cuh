@@ -1,6 +1,8 @@
 // rc_march.cuh -- the persistent march kernel (kernel_fluid + march_ray +
 // kernel_surface of src/montecarlo/mc_gpu_noint.cu, restructured for SIMT).
 #pragma once
+#include <type_traits>
+
 #include "rc_device.cuh"
 
 namespace rc {
@@ -118,10 +120,15 @@ __global__ void k_prio_tiles(const DSolve<R> *Sp, float thr, const float *kmin, 
     }
 }
 
-template <typename R>
+template <typename E>
 struct WarpShared {
-    Emitted<R> ring[kRing];
+    E ring[kRing];
 };
+
+// Ring entry of the march: the emitted bundle, plus its counter words and
+// first free path when the medium scatters.
+template <typename R, bool SCAT>
+using RingEntry = typename std::conditional<SCAT, EmittedScat<R>, Emitted<R>>::type;
 
 // Index of the solve owning a global tile (tile_start is an exclusive prefix).
 __device__ __forceinline__ int solve_of_tile(const long long *tile_start, int nsolves, unsigned long long tile) {
@@ -149,13 +156,15 @@ __device__ __forceinline__ void flush_counters(DScalars *sc, unsigned long long 
 }
 
 // MINB: resident 256-thread blocks per SM the register allocation must
-// allow (2: up to 128 registers, 3: 80, 4: 64).
-template <typename R, int MINB>
+// allow (2: up to 128 registers, 3: 80, 4: 64).  SCAT: the variant for
+// media with scattering particles (solves without them run in it unchanged).
+template <typename R, int MINB, bool SCAT>
 __global__ void __launch_bounds__(256, MINB) k_march(MarchArgs a) {
+    using Entry = RingEntry<R, SCAT>;
     extern __shared__ __align__(16) unsigned char smem[];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
-    WarpShared<R> *ws = reinterpret_cast<WarpShared<R> *>(smem) + warp;
-    const size_t wbytes = ((sizeof(WarpShared<R>) * nwarps) + 15) & ~(size_t)15;
+    WarpShared<Entry> *ws = reinterpret_cast<WarpShared<Entry> *>(smem) + warp;
+    const size_t wbytes = ((sizeof(WarpShared<Entry>) * nwarps) + 15) & ~(size_t)15;
     const int pool_max = kWarp * a.rpt_max;
     double *slots0 = reinterpret_cast<double *>(smem + wbytes) + (size_t)warp * 2 * pool_max;
     const DSolve<R> *solves = reinterpret_cast<const DSolve<R> *>(a.solves);
@@ -187,6 +196,7 @@ __global__ void __launch_bounds__(256, MINB) k_march(MarchArgs a) {
     int myb = 0, mypar = 0;
     unsigned long long nsteps = 0, nbund = 0;
     Ray<R> r;
+    ScatState<R> qs;
 
     for (;;) {
         // ---- fetch the next tile into a free buffer
@@ -268,7 +278,8 @@ __global__ void __launch_bounds__(256, MINB) k_march(MarchArgs a) {
         // ---- converged emission wave: one bundle per lane
         if (count < kWarp && epar >= 0 && !((emitted >> epar) & 1u)) {
             const int b = next_b + lane;
-            Emitted<R> e;
+            Entry ee;
+            Emitted<R> &e = entry_base(ee);
             bool ok = false;
             if (b < pool) {
                 const ItemId it = decode_item(S, (epar ? item0_1 : item0_0) + (b >> lrpt));
@@ -277,6 +288,7 @@ __global__ void __launch_bounds__(256, MINB) k_march(MarchArgs a) {
                     nbund++;
                     ok = emit_bundle(e, S, it.kind, it.i, it.j, it.k, it.v, h);
                     e.kk |= (b << 18) | (epar << 29);
+                    if constexpr (SCAT) scatter_start(ee.cx, ee.cy, ee.cz, ee.tau, S, it.kind, it.i, it.j, it.k, it.v, h);
                 }
             }
             const unsigned m = __ballot_sync(0xffffffffu, ok);
@@ -301,7 +313,7 @@ __global__ void __launch_bounds__(256, MINB) k_march(MarchArgs a) {
                 }
                 pos = rank;
             }
-            if (ok) ws->ring[(head + count + pos) & (kRing - 1)] = e;
+            if (ok) ws->ring[(head + count + pos) & (kRing - 1)] = ee;
             count += __popc(m);
             if (epar) out1 += __popc(m);
             else out0 += __popc(m);
@@ -317,8 +329,10 @@ __global__ void __launch_bounds__(256, MINB) k_march(MarchArgs a) {
             if (!active) {
                 const int rank = __popc(m & lt);
                 if (rank < navail) {
-                    const Emitted<R> &e = ws->ring[(head + rank) & (kRing - 1)];
+                    const Entry &ee = ws->ring[(head + rank) & (kRing - 1)];
+                    const Emitted<R> &e = entry_base(ee);
                     place_bundle(r, S, e);
+                    if constexpr (SCAT) place_scatter(qs, S, ee);
                     myb = (e.kk >> 18) & 0x7ff;
                     mypar = (e.kk >> 29) & 1;
                     took = true;
@@ -352,7 +366,7 @@ __global__ void __launch_bounds__(256, MINB) k_march(MarchArgs a) {
             for (;;) {
                 bool fin = false;
                 if (active) {
-                    const int budget = march_step(r, S);
+                    const int budget = march_step<R, SCAT>(r, qs, S);
                     nsteps++;
                     bool done = !(r.tra > r.tol);
                     if (!done && r.counter >= budget) done = !level_advance(r, S);
@@ -401,9 +415,9 @@ __global__ void __launch_bounds__(256, MINB) k_march(MarchArgs a) {
     if (cur_solve >= 0) flush_counters(Sp->sc, nsteps, nbund, lane);
 }
 
-template <typename R>
+template <typename R, bool SCAT>
 constexpr size_t march_smem_bytes(int block, int rpt_max) {
-    return ((((size_t)sizeof(WarpShared<R>) * (block / kWarp)) + 15) & ~(size_t)15) +
+    return ((((size_t)sizeof(WarpShared<RingEntry<R, SCAT>>) * (block / kWarp)) + 15) & ~(size_t)15) +
            (size_t)(block / kWarp) * 2 * kWarp * rpt_max * sizeof(double);
 }
 

@@ -89,6 +89,57 @@ int rc_tables_view(const rc_table_set *ts, rc_tables *view) {
 
 void rc_tables_free(rc_table_set *ts) { delete ts; }
 
+int rc_scattering_synthetic(const rc_scatter_spec *spec, rc_scatter_set **out) {
+    if (!spec || !out) return set_err(nullptr, RC_E_INVALID, "NULL argument");
+    auto *s = new rc_scatter_set();
+    std::string err;
+    const int rc = scattering_synthetic(*spec, s->s, err);
+    if (rc) {
+        delete s;
+        return set_err(nullptr, rc, err);
+    }
+    *out = s;
+    return RC_OK;
+}
+
+int rc_scattering_read_dir(const char *dir, int nB, int nQ, rc_scatter_set **out) {
+    if (!dir || !out) return set_err(nullptr, RC_E_INVALID, "NULL argument");
+    auto *s = new rc_scatter_set();
+    std::string err;
+    const int rc = scattering_read_dir(dir, nB, nQ, s->s, err);
+    if (rc) {
+        delete s;
+        return set_err(nullptr, rc, err);
+    }
+    *out = s;
+    return RC_OK;
+}
+
+int rc_scattering_write_dir(const rc_scatter_set *s, const char *dir) {
+    if (!s || !dir) return set_err(nullptr, RC_E_INVALID, "NULL argument");
+    std::string err;
+    const int rc = scattering_write_dir(s->s, dir, err);
+    if (rc) return set_err(nullptr, rc, err);
+    return RC_OK;
+}
+
+int rc_scattering_validate(const rc_scattering *s, char *msg, size_t msglen) {
+    if (!s) return set_err(nullptr, RC_E_INVALID, "NULL particle tables");
+    std::string err;
+    const int rc = scattering_check(*s, err);
+    if (msg && msglen) snprintf(msg, msglen, "%s", err.c_str());
+    if (rc) return set_err(nullptr, rc, err);
+    return RC_OK;
+}
+
+int rc_scattering_view(const rc_scatter_set *s, rc_scattering *view) {
+    if (!s || !view) return set_err(nullptr, RC_E_INVALID, "NULL argument");
+    s->s.view(view);
+    return RC_OK;
+}
+
+void rc_scattering_free(rc_scatter_set *s) { delete s; }
+
 int rc_grid_level(const rc_params *p, int level, float *xu, float *yu, float *zu, float *x, float *y, float *z) {
     if (!p) return set_err(nullptr, RC_E_INVALID, "NULL params");
     std::string err;
@@ -163,6 +214,12 @@ int rc_set_tables(rc_ctx *c, const rc_tables *t) {
     TableSet ts;
     ts.from_view(t);
     return with_impl(c, [&](auto &im) { return im.set_tables(ts); });
+}
+
+int rc_set_scattering(rc_ctx *c, const rc_scattering *s) {
+    if (!c) return set_err(nullptr, RC_E_INVALID, "NULL context");
+    cudaSetDevice(c->device);
+    return with_impl(c, [&](auto &im) { return im.set_scattering(s); });
 }
 
 int rc_solve_async(rc_ctx *c, const float *T, int zstart, rc_ticket *ticket) {
@@ -355,12 +412,13 @@ int batch_enqueue(rc_batch *b) {
     int rc = batch_reserve<R>(b, n);
     if (rc) return rc;
     DSolve<R> *hs = static_cast<DSolve<R> *>(b->h_solves);
-    int rpt_max = 1, block = 256;
+    int rpt_max = 1, block = 256, scat = 0;
     long long max_cells = 1;
     b->h_tiles[0] = 0;
     for (size_t i = 0; i < n; ++i) {
         rc_ctx *c = b->m[i].ctx;
         Impl<R> &im = *static_cast<Impl<R> *>(c->impl);
+        if (im.nA > 0) scat = 1;  // the scattering variant of the march serves every member
         Slot<R> &s = *static_cast<Slot<R> *>(b->m[i].slot);
         rc = im.prepare(s, nullptr, b->m[i].zstart, c->rpt, b->st);
         if (rc) return set_err(err_, rc, c->err);
@@ -381,7 +439,7 @@ int batch_enqueue(rc_batch *b) {
     RC_CK(cudaMemcpyAsync(b->d_outs, b->h_outs, n * sizeof(TallyOut), cudaMemcpyHostToDevice, b->st));
     Impl<R> &im0 = *static_cast<Impl<R> *>(b->m[0].ctx->impl);
     rc = im0.launch_march(static_cast<const DSolve<R> *>(b->d_solves), b->d_tiles, (int)n, b->h_tiles[n],
-                          b->d_counter, block, rpt_max, b->st);
+                          b->d_counter, block, rpt_max, b->st, 0, nullptr, scat);
     if (rc) return set_err(err_, rc, b->m[0].ctx->err);
     rc = im0.launch_tally(static_cast<const DSolve<R> *>(b->d_solves), b->d_outs, (int)n, max_cells, b->st);
     if (rc) return set_err(err_, rc, b->m[0].ctx->err);

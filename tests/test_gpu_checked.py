@@ -2,7 +2,8 @@
 table, field and partial-sum index of the march is checked against its
 array on the device.  Small cases covering each path (grey, narrow band
 with levels, every wall type, both wall fluxes, a z slab, band-sorted
-order, the FP64 build, a batch, the server, the allocation-free solve) run
+order, the FP64 build, particle scattering, a batch, the server, the
+allocation-free solve) run
 in a child process that loads the checked library; none may flag an index
 (status bit 3) and each result must equal the oracle bit for bit."""
 import json
@@ -32,6 +33,8 @@ def _cases():
     p = W.channel_params(16, 8, 8, photmax=16, nVar=2, calcwalls=1, adiabw=1, **lv)
     p.p_col = 2
     out.append(("z_slab", p, tabs, {"zstart": 5}))
+    out.append(("scattering", W.channel_params(16, 8, 8, photmax=16, nVar=2, bd_y=3, calcwalls=1, adiabw=1,
+                                               adiabe=1, **lv), tabs, {"scatter": 1}))
     return out
 
 
@@ -47,11 +50,16 @@ def child():
         s = api.Solver(p, tabs)
         if opt.get("sort"):
             s.set_launch(sort_bands=1)
+        sc = None
+        if opt.get("scatter"):
+            sc = api.Scattering.synthetic(nB=24, nQ=4, nA=61, ksca_lo=0.3, ksca_hi=5.0, g_lo=-0.3, g_hi=0.8)
+            s.set_scattering(sc)
         z = opt.get("zstart", 1)
         t = s.solve_async(T, zstart=z)
         st = s.info(t).status
         r = s.collect(t)
-        o = O.solve(p, tabs, T, zstart=z, rpt=s.get_launch()[0], fp64=bool(p.floatpoint))
+        o = O.solve(p, tabs, T, zstart=z, rpt=s.get_launch()[0], fp64=bool(p.floatpoint),
+                    scatter=sc.arrays() if sc is not None else None)
         res[name] = dict(status=st, equal=bool(np.array_equal(r.q64, o["q64"]) and np.array_equal(r.qw64, o["qw64"])))
         s.close()
     # a batch of two problems and a served request
@@ -107,7 +115,7 @@ def test_checked_build_flags_nothing_and_matches_the_oracle():
                        capture_output=True, text=True, timeout=900)
     assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-4000:]
     res = json.loads(r.stdout.strip().splitlines()[-1])
-    assert len(res) == 10
+    assert len(res) == 11
     for name, v in res.items():
         assert v["status"] >= 0, (name, v)
         assert v["status"] & 8 == 0, (name, v["status"] >> 8)
