@@ -521,17 +521,27 @@ def leg_batched(dev, passes=2, tol=None, max_bundles=2.5e11, served=True, warm=T
     for it in items:
         b.add(it["s"], it["T"])
 
+    host_collect = []
+
     def batched_pass():
         t0 = time.perf_counter()
         b.run()
         b.wait()
+        t1 = time.perf_counter()
         for i, it in enumerate(items):
             b.collect_into(i, it["Q"], it["S"])
-        return time.perf_counter() - t0
+        t2 = time.perf_counter()
+        host_collect.append(t2 - t1)
+        return t2 - t0
 
     if warm:
         batched_pass()
     t_batch = min(batched_pass() for _ in range(passes))
+    ph = b.phases()
+    phases = {"setup_ms": ph[0], "march_ms": ph[1], "tally_and_copies_ms": ph[2],
+              "host_collect_ms": 1000 * min(host_collect),
+              "note": "device phases of the last batched run (CUDA events in the graph); host_collect is the "
+                      "Fortran-layout scatter of all members after the wait"}
     identical = all(np.array_equal(r, it["Q"]) for r, it in zip(ref, items))
     b.close()
     if not served:
@@ -544,7 +554,7 @@ def leg_batched(dev, passes=2, tol=None, max_bundles=2.5e11, served=True, warm=T
                 "batched_vs_plain": t_plain / t_batch, "plain_bundles_per_s": bundles / t_plain,
                 "batched_bundles_per_s": bundles / t_batch, "steps_per_pass": steps,
                 "plain_steps_per_s": steps / t_plain, "batched_steps_per_s": steps / t_batch,
-                "batched_equals_plain": identical,
+                "batched_phases": phases, "batched_equals_plain": identical,
                 "timing": "wall clock per pass of all solves, host arrays in/out, best of %d after one warm-up "
                           "pass" % passes}
     srv = api.Server(device=dev, max_inflight=len(items))
@@ -574,8 +584,9 @@ def leg_batched(dev, passes=2, tol=None, max_bundles=2.5e11, served=True, warm=T
             "plain_bundles_per_s": bundles / t_plain, "batched_bundles_per_s": bundles / t_batch,
             "steps_per_pass": steps, "steps_per_bundle": steps / bundles,
             "plain_steps_per_s": steps / t_plain, "batched_steps_per_s": steps / t_batch,
-            "batched_equals_plain": identical, "timing": "wall clock per pass of all solves, host arrays in/out, "
-                                                        "best of %d" % passes}
+            "batched_phases": phases, "batched_equals_plain": identical,
+            "timing": "wall clock per pass of all solves, host arrays in/out, "
+                      "best of %d" % passes}
 
 
 def serve_run(dev, n_requests, load, inflight=32, policy="srpt", wall_cap=None, seed=2024):

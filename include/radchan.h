@@ -394,11 +394,20 @@ int rc_probe_gather(int device, size_t bytes, int mode, int iters, double *secto
 typedef struct rc_batch rc_batch;
 /* A batch runs many contexts' solves (uneven grids, tables, photmax) in
  * one persistent work-queue launch; with use_graph the whole sequence
- * (copies + kernels) is captured once and replayed. */
+ * (copies + kernels) is captured once and replayed.  The long-ray priority
+ * list (rc_set_priority) spans the whole batch when any member has it on
+ * and the batch has at most 2^22 tiles: the march claims the tiles of every
+ * member that hold a long ray first.  Every run also gathers the members'
+ * float results (Q, sigma, wall fluxes) into one buffer copied to the host
+ * once, so rc_batch_collect with only Q / sigma copies nothing more. */
 int rc_batch_create(int device, int use_graph, rc_batch **out);
 int rc_batch_add(rc_batch *b, rc_ctx *ctx, const float *T_host, int zstart);
 int rc_batch_run(rc_batch *b);          /* enqueue; returns at once */
 int rc_batch_wait(rc_batch *b, float *ms_device);
+/* Device time of the last run by phase: set-up of every member (field
+ * copies, set-up kernels, priority list), the march, and tally plus result
+ * copies.  Waits for the run. */
+int rc_batch_phases(rc_batch *b, float *ms_setup, float *ms_march, float *ms_tally);
 int rc_batch_collect(rc_batch *b, int index, float *Q, float *sigma,
                      double *q64, double *var64, double *qw64, double *vw64);
 int rc_batch_destroy(rc_batch *b);

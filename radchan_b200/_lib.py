@@ -158,6 +158,7 @@ _SIGS = [
     ("rc_batch_add", _I, [_VP, _VP, _FP, _I]),
     ("rc_batch_run", _I, [_VP]),
     ("rc_batch_wait", _I, [_VP, C.POINTER(C.c_float)]),
+    ("rc_batch_phases", _I, [_VP, C.POINTER(C.c_float), C.POINTER(C.c_float), C.POINTER(C.c_float)]),
     ("rc_batch_collect", _I, [_VP, _I, _FP, _FP, _DP, _DP, _DP, _DP]),
     ("rc_batch_destroy", _I, [_VP]),
     ("rc_server_create", _I, [_I, C.c_double, _I, C.POINTER(_VP)]),

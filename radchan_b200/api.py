@@ -469,6 +469,12 @@ class Batch:
         L.check(L.lib().rc_batch_wait(self.h, C.byref(ms)))
         return ms.value
 
+    def phases(self):
+        """Device ms of the last run: (set-up, march, tally + copies)."""
+        a, b, c = C.c_float(), C.c_float(), C.c_float()
+        L.check(L.lib().rc_batch_phases(self.h, C.byref(a), C.byref(b), C.byref(c)))
+        return a.value, b.value, c.value
+
     def collect(self, index, want64=True) -> Result:
         s, _ = self.members[index]
         p = s.p

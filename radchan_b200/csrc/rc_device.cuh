@@ -543,6 +543,7 @@ struct ScatState {
     int nev;              // scattering events so far
     R ks;                 // scattering coefficient of the bundle's band and g point
     R tau;                // optical depth left to the next event
+    bool turn;            // stopped at an event, new direction not drawn yet
 };
 
 // A ring entry of a scattering medium: the emitted bundle, its counter
@@ -640,6 +641,7 @@ __device__ __forceinline__ void place_scatter(ScatState<R> &q, const DSolve<R> &
     q.cz = e.cz;
     q.tau = e.tau;
     q.nev = 0;
+    q.turn = false;
     const int nb = e.e.nbg & 0xfffff, g = e.e.nbg >> 20;
     q.ks = (S.nA > 0) ? S.ksca[RC_IX((size_t)nb * S.nQ + g, (long long)S.nB * S.nQ, SITE_KSCA, S)] : (R)0;
 }
@@ -661,7 +663,11 @@ __device__ __forceinline__ const Emitted<R> &entry_base(const EmittedScat<R> &e)
 // direction component (never 0: emission floors it at 1e-10).  With SCAT, a
 // bundle whose scattering optical depth over the step exceeds what is left
 // to its next event stops at the event inside the cell (absorbing along
-// the shortened path), turns, and counts the event as a step.
+// the shortened path), counts the event as a step and sets qs.turn: the
+// caller draws the new direction (scatter_turn) before the next step.  The
+// turn depends neither on the cell nor on the level, so a caller may
+// advance the level first and gather the turns of several lanes into one
+// pass.
 template <typename R, bool SCAT>
 __device__ __forceinline__ int march_step(Ray<R> &r, ScatState<R> &qs, const DSolve<R> &S) {
     // S lives in global memory (read-only during every kernel that steps)
@@ -696,7 +702,7 @@ __device__ __forceinline__ int march_step(Ray<R> &r, ScatState<R> &qs, const DSo
             r.yp = RT<R>::fma_(dsc, r.sy, r.yp);
             r.zp = RT<R>::fma_(dsc, r.sz, r.zp);
             absorb(r, dsc, absco, blackpow);
-            scatter_turn(r, qs, S);
+            qs.turn = true;
             r.counter += 1;
             return B.w;
         }

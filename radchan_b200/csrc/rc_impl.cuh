@@ -154,6 +154,18 @@ struct ImplBase {
     virtual ~ImplBase() {}
 };
 
+// Gather of float result arrays into one buffer: segment blockIdx.y copies
+// n floats from src to dst + off (batch results, one copy to the host).
+struct PackSeg {
+    const float *src;
+    long long off, n;
+};
+static __global__ void k_pack(const PackSeg *segs, float *dst) {
+    const PackSeg s = segs[blockIdx.y];
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < s.n; i += (long long)gridDim.x * blockDim.x)
+        dst[s.off + i] = s.src[i];
+}
+
 struct SlotCommon {
     cudaStream_t st = nullptr;
     cudaEvent_t e0 = nullptr, e1 = nullptr, e_march0 = nullptr, e_march1 = nullptr;
@@ -1200,7 +1212,32 @@ struct Impl : ImplBase {
     }
 
     // Fortran layout (0:imax+1, 0:jmax+1, 0:kloc+1) (mc_gpu_noint.cu:975-1005).
-    void scatter(Slot<R> &s, float *Q, float *sigma) {
+    void scatter(Slot<R> &s, float *Q, float *sigma) { scatter_from(s.h_Qc, s.h_Sc, s.h_Wq, s.h_Ws, Q, sigma); }
+
+    // Float results of a batch member from the batch's packed host copy
+    // (Q, sigma, wall flux, wall sigma one after the other at `pack`).
+    int collect_packed(Slot<R> &s, const float *pack, float *Q, float *sigma) {
+        std::string *err_ = &c->err;
+        RC_FAILPOINT("collect");
+        const size_t ncf = (size_t)c->p.imax * c->p.jmax * c->kloc;
+        const size_t nwc = (size_t)2 * c->p.jmax * c->kloc;
+        scatter_from(pack, pack + ncf, pack + 2 * ncf, pack + 2 * ncf + nwc, Q, sigma);
+        if (s.h_sc->status & 2) return set_err(err_, RC_E_RANGE, "temperature field contains non-finite values");
+        return RC_OK;
+    }
+    size_t packed_floats() const {
+        return (size_t)2 * c->p.imax * c->p.jmax * c->kloc + (size_t)4 * c->p.jmax * c->kloc;
+    }
+    void pack_segments(Slot<R> &s, long long off, PackSeg *seg) const {
+        const long long ncf = (long long)c->p.imax * c->p.jmax * c->kloc;
+        const long long nwc = 2LL * c->p.jmax * c->kloc;
+        seg[0] = PackSeg{s.d_Qc, off, ncf};
+        seg[1] = PackSeg{s.d_Sc, off + ncf, ncf};
+        seg[2] = PackSeg{s.d_Wq, off + 2 * ncf, nwc};
+        seg[3] = PackSeg{s.d_Ws, off + 2 * ncf + nwc, nwc};
+    }
+
+    void scatter_from(const float *Qc, const float *Sc, const float *Wq, const float *Ws, float *Q, float *sigma) {
         const rc_params &p = c->p;
         const int im = p.imax, jm = p.jmax, kl = c->kloc;
         const size_t sx = (size_t)im + 2, sy = (size_t)jm + 2;
@@ -1208,19 +1245,19 @@ struct Impl : ImplBase {
             for (int j = 1; j <= jm; ++j) {
                 const size_t src = ((size_t)(k - 1) * jm + (j - 1)) * im;
                 const size_t dst = sx * ((size_t)j + sy * k);
-                if (Q) memcpy(Q + dst + 1, s.h_Qc + src, im * sizeof(float));
-                if (sigma) memcpy(sigma + dst + 1, s.h_Sc + src, im * sizeof(float));
+                if (Q) memcpy(Q + dst + 1, Qc + src, im * sizeof(float));
+                if (sigma) memcpy(sigma + dst + 1, Sc + src, im * sizeof(float));
                 if (p.adiabw || p.adiabe) {
                     const size_t w = (size_t)(k - 1) * jm + (j - 1);
                     const size_t e = (size_t)jm * kl + w;
                     const bool cw = p.calcwalls && p.adiabw, ce = p.calcwalls && p.adiabe;
                     if (Q) {
-                        Q[dst] = cw ? s.h_Wq[w] : 0.f;
-                        Q[dst + im + 1] = ce ? s.h_Wq[e] : 0.f;
+                        Q[dst] = cw ? Wq[w] : 0.f;
+                        Q[dst + im + 1] = ce ? Wq[e] : 0.f;
                     }
                     if (sigma) {
-                        sigma[dst] = cw ? s.h_Ws[w] : 0.f;
-                        sigma[dst + im + 1] = ce ? s.h_Ws[e] : 0.f;
+                        sigma[dst] = cw ? Ws[w] : 0.f;
+                        sigma[dst + im + 1] = ce ? Ws[e] : 0.f;
                     }
                 }
             }

@@ -339,6 +339,10 @@ __global__ void k_trace(const DSolve<R> *Sp, int n, const rc_bundle_id *ids, rc_
                 c[3] = r.kc;
             }
             march_step<R, SCAT>(r, qs, S);
+            if (SCAT && qs.turn) {
+                scatter_turn(r, qs, S);
+                qs.turn = false;
+            }
             ns++;
             active = r.tra > r.tol;
             if (active) active = level_advance(r, S);

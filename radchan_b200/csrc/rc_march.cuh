@@ -365,7 +365,9 @@ __global__ void __launch_bounds__(256, MINB) k_march(MarchArgs a) {
                 (!drained && (epar < 0 || (((emitted >> epar) & 1u) && !((busy >> (epar ^ 1)) & 1u))));
             for (;;) {
                 bool fin = false;
-                if (active) {
+                bool wait_turn = false;
+                if constexpr (SCAT) wait_turn = active && qs.turn;
+                if (active && !wait_turn) {
                     const int budget = march_step<R, SCAT>(r, qs, S);
                     nsteps++;
                     bool done = !(r.tra > r.tol);
@@ -374,7 +376,9 @@ __global__ void __launch_bounds__(256, MINB) k_march(MarchArgs a) {
                         slots0[mypar * pool_max + myb] = r.De;
                         active = false;
                         fin = true;
+                        if constexpr (SCAT) qs.turn = false;
                     }
+                    if constexpr (SCAT) wait_turn = active && qs.turn;
                 }
                 const unsigned fm = __ballot_sync(0xffffffffu, fin);
                 if (fm) {
@@ -383,10 +387,21 @@ __global__ void __launch_bounds__(256, MINB) k_march(MarchArgs a) {
                     out0 -= __popc(fm) - n1;
                     amask &= ~fm;
                 }
-                const int nidle = kWarp - __popc(amask);
+                // lanes stopped at a scattering event wait for the warp's next
+                // turn pass, which draws all their new directions at once
+                unsigned tm = 0u;
+                if constexpr (SCAT) tm = __ballot_sync(0xffffffffu, wait_turn);
+                const int nidle = kWarp - __popc(amask & ~tm);
                 if (nidle == kWarp) break;
-                if (nidle >= kFeedIdle && can_feed) break;
+                if (nidle >= kFeedIdle && (can_feed || tm)) break;
                 if (fm && ((((busy & emitted) & 1u) && out0 == 0) || (((busy & emitted) & 2u) && out1 == 0))) break;
+            }
+        }
+        // ---- scattering: the new directions of every lane stopped at an event
+        if constexpr (SCAT) {
+            if (active && qs.turn) {
+                scatter_turn(r, qs, S);
+                qs.turn = false;
             }
         }
         // ---- reduce finished tiles: chunk sums in bundle order, group sums

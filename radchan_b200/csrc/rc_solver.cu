@@ -370,6 +370,8 @@ struct rc_batch {
     std::vector<Member> m;
     cudaStream_t st = nullptr;
     cudaEvent_t e0 = nullptr, e1 = nullptr;
+    // end of the set-up of every member, end of the march (phase timing)
+    cudaEvent_t e_setup = nullptr, e_march = nullptr;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     bool built = false;
@@ -378,6 +380,17 @@ struct rc_batch {
     TallyOut *d_outs = nullptr, *h_outs = nullptr;
     unsigned long long *d_counter = nullptr;
     size_t cap = 0;
+    // the members' float results gathered into one buffer and copied to
+    // the host once per run (k_pack + one cudaMemcpyAsync)
+    PackSeg *d_segs = nullptr, *h_segs = nullptr;
+    float *d_pack = nullptr, *h_pack = nullptr;
+    size_t pack_cap = 0;
+    std::vector<size_t> pack_off;
+    // members' set-up chains run side by side on kSideStreams streams (forked
+    // from and joined back into st: parallel branches of the captured graph)
+    static constexpr int kSideStreams = 16;
+    cudaStream_t side[kSideStreams] = {};
+    cudaEvent_t fork = nullptr, join[kSideStreams] = {};
     std::string err;
 };
 
@@ -386,6 +399,7 @@ namespace {
 template <typename R>
 int batch_reserve(rc_batch *b, size_t n) {
     std::string *err_ = &b->err;
+    if (4 * n > 65535) return set_err(err_, RC_E_INVALID, "more than 16383 solves in one batch");
     if (n <= b->cap) return RC_OK;
     if (b->d_solves) cudaFree(b->d_solves);
     if (b->h_solves) cudaFreeHost(b->h_solves);
@@ -399,15 +413,48 @@ int batch_reserve(rc_batch *b, size_t n) {
     RC_CK(cudaHostAlloc((void **)&b->h_tiles, (n + 1) * sizeof(long long), cudaHostAllocDefault));
     RC_CK(cudaMalloc((void **)&b->d_outs, n * sizeof(TallyOut)));
     RC_CK(cudaHostAlloc((void **)&b->h_outs, n * sizeof(TallyOut), cudaHostAllocDefault));
+    if (b->d_segs) cudaFree(b->d_segs);
+    if (b->h_segs) cudaFreeHost(b->h_segs);
+    b->d_segs = b->h_segs = nullptr;
+    RC_CK(cudaMalloc((void **)&b->d_segs, 4 * n * sizeof(PackSeg)));
+    RC_CK(cudaHostAlloc((void **)&b->h_segs, 4 * n * sizeof(PackSeg), cudaHostAllocDefault));
     b->cap = n;
+    return RC_OK;
+}
+
+// The packed-results buffer, sized by the members' problems (allocated
+// before any capture).
+template <typename R>
+int batch_reserve_members(rc_batch *b) {
+    std::string *err_ = &b->err;
+    size_t floats = 0;
+    b->pack_off.assign(b->m.size(), 0);
+    for (size_t i = 0; i < b->m.size(); ++i) {
+        Impl<R> &im = *static_cast<Impl<R> *>(b->m[i].ctx->impl);
+        b->pack_off[i] = floats;
+        floats += im.packed_floats();
+    }
+    if (floats > b->pack_cap) {
+        if (b->d_pack) cudaFree(b->d_pack);
+        if (b->h_pack) cudaFreeHost(b->h_pack);
+        b->d_pack = b->h_pack = nullptr;
+        b->pack_cap = 0;
+        RC_CK(cudaMalloc((void **)&b->d_pack, floats * sizeof(float)));
+        RC_CK(cudaHostAlloc((void **)&b->h_pack, floats * sizeof(float), cudaHostAllocDefault));
+        b->pack_cap = floats;
+    }
     return RC_OK;
 }
 
 // The whole batch on b->st: per member field copy + set-up, one march
 // over every member's tiles, one tally launch, scalars back.
 template <typename R>
-int batch_enqueue(rc_batch *b) {
+int batch_enqueue(rc_batch *b, bool capturing) {
     std::string *err_ = &b->err;
+    // phase events: inside a captured graph they become event-record nodes
+    auto mark = [&](cudaEvent_t ev) {
+        return capturing ? cudaEventRecordWithFlags(ev, b->st, cudaEventRecordExternal) : cudaEventRecord(ev, b->st);
+    };
     const size_t n = b->m.size();
     int rc = batch_reserve<R>(b, n);
     if (rc) return rc;
@@ -415,13 +462,23 @@ int batch_enqueue(rc_batch *b) {
     int rpt_max = 1, block = 256, scat = 0;
     long long max_cells = 1;
     b->h_tiles[0] = 0;
-    for (size_t i = 0; i < n; ++i) {
+    // every member's field copy and set-up kernels, round-robin over the side
+    // streams: independent chains that run side by side (a member's chain is
+    // a dozen small launches; one after another they took ~110 us each)
+    const int ns = (int)std::min<size_t>(n, (size_t)rc_batch::kSideStreams);
+    RC_CK(cudaEventRecord(b->fork, b->st));
+    for (int k = 0; k < ns; ++k) RC_CK(cudaStreamWaitEvent(b->side[k], b->fork, 0));
+    int rc_members = RC_OK;
+    for (size_t i = 0; i < n && !rc_members; ++i) {
         rc_ctx *c = b->m[i].ctx;
         Impl<R> &im = *static_cast<Impl<R> *>(c->impl);
         if (im.nA > 0) scat = 1;  // the scattering variant of the march serves every member
         Slot<R> &s = *static_cast<Slot<R> *>(b->m[i].slot);
-        rc = im.prepare(s, nullptr, b->m[i].zstart, c->rpt, b->st);
-        if (rc) return set_err(err_, rc, c->err);
+        rc = im.prepare(s, nullptr, b->m[i].zstart, c->rpt, b->side[i % ns]);
+        if (rc) {
+            rc_members = set_err(err_, rc, c->err);
+            break;
+        }
         hs[i] = *s.h_desc;
         b->h_outs[i] = *s.h_out;
         b->h_tiles[i + 1] = b->h_tiles[i] + s.h_desc->n_tiles;
@@ -429,6 +486,11 @@ int batch_enqueue(rc_batch *b) {
         if (i == 0) block = c->block;
         max_cells = std::max(max_cells, im.tally_cells());
     }
+    for (int k = 0; k < ns; ++k) {
+        RC_CK(cudaEventRecord(b->join[k], b->side[k]));
+        RC_CK(cudaStreamWaitEvent(b->st, b->join[k], 0));
+    }
+    if (rc_members) return rc_members;
     // descriptors with their run-time fields already patched on the device
     for (size_t i = 0; i < n; ++i) {
         Slot<R> &s = *static_cast<Slot<R> *>(b->m[i].slot);
@@ -438,11 +500,30 @@ int batch_enqueue(rc_batch *b) {
     RC_CK(cudaMemcpyAsync(b->d_tiles, b->h_tiles, (n + 1) * sizeof(long long), cudaMemcpyHostToDevice, b->st));
     RC_CK(cudaMemcpyAsync(b->d_outs, b->h_outs, n * sizeof(TallyOut), cudaMemcpyHostToDevice, b->st));
     Impl<R> &im0 = *static_cast<Impl<R> *>(b->m[0].ctx->impl);
+    RC_CK(mark(b->e_setup));
     rc = im0.launch_march(static_cast<const DSolve<R> *>(b->d_solves), b->d_tiles, (int)n, b->h_tiles[n],
                           b->d_counter, block, rpt_max, b->st, 0, nullptr, scat);
     if (rc) return set_err(err_, rc, b->m[0].ctx->err);
+    RC_CK(mark(b->e_march));
     rc = im0.launch_tally(static_cast<const DSolve<R> *>(b->d_solves), b->d_outs, (int)n, max_cells, b->st);
     if (rc) return set_err(err_, rc, b->m[0].ctx->err);
+    // float results of every member into one buffer, one copy to the host
+    long long maxn = 1;
+    for (size_t i = 0; i < n; ++i) {
+        Impl<R> &im = *static_cast<Impl<R> *>(b->m[i].ctx->impl);
+        im.pack_segments(*static_cast<Slot<R> *>(b->m[i].slot), (long long)b->pack_off[i], b->h_segs + 4 * i);
+        for (int q = 0; q < 4; ++q) maxn = std::max(maxn, b->h_segs[4 * i + q].n);
+    }
+    size_t floats = 0;
+    for (size_t i = 0; i < n; ++i)
+        floats += static_cast<Impl<R> *>(b->m[i].ctx->impl)->packed_floats();
+    RC_CK(cudaMemcpyAsync(b->d_segs, b->h_segs, 4 * n * sizeof(PackSeg), cudaMemcpyHostToDevice, b->st));
+    {
+        const int gx = (int)std::min<long long>((maxn + 255) / 256, 64);
+        k_pack<<<dim3(gx, (unsigned)(4 * n)), 256, 0, b->st>>>(b->d_segs, b->d_pack);
+        RC_CK(cudaGetLastError());
+    }
+    RC_CK(cudaMemcpyAsync(b->h_pack, b->d_pack, floats * sizeof(float), cudaMemcpyDeviceToHost, b->st));
     for (size_t i = 0; i < n; ++i) {
         Slot<R> &s = *static_cast<Slot<R> *>(b->m[i].slot);
         RC_CK(cudaMemcpyAsync(s.h_sc, s.d_sc, sizeof(DScalars), cudaMemcpyDeviceToHost, b->st));
@@ -499,6 +580,13 @@ int rc_batch_create(int device, int use_graph, rc_batch **out) {
     if ((e = cudaStreamCreateWithFlags(&b->st, cudaStreamNonBlocking)) != cudaSuccess) return fail(e);
     if ((e = cudaEventCreate(&b->e0)) != cudaSuccess) return fail(e);
     if ((e = cudaEventCreate(&b->e1)) != cudaSuccess) return fail(e);
+    if ((e = cudaEventCreate(&b->e_setup)) != cudaSuccess) return fail(e);
+    if ((e = cudaEventCreate(&b->e_march)) != cudaSuccess) return fail(e);
+    if ((e = cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming)) != cudaSuccess) return fail(e);
+    for (int k = 0; k < rc_batch::kSideStreams; ++k) {
+        if ((e = cudaStreamCreateWithFlags(&b->side[k], cudaStreamNonBlocking)) != cudaSuccess) return fail(e);
+        if ((e = cudaEventCreateWithFlags(&b->join[k], cudaEventDisableTiming)) != cudaSuccess) return fail(e);
+    }
     if ((e = cudaMalloc((void **)&b->d_counter, sizeof(unsigned long long))) != cudaSuccess) return fail(e);
     (void)err_;
     *out = b;
@@ -542,9 +630,13 @@ int rc_batch_run(rc_batch *b) {
     // all allocations happen before any stream capture
     rc = b->dbl ? batch_reserve<double>(b, b->m.size()) : batch_reserve<float>(b, b->m.size());
     if (rc) return rc;
+    if (!b->built || !b->use_graph) {
+        rc = b->dbl ? batch_reserve_members<double>(b) : batch_reserve_members<float>(b);
+        if (rc) return rc;
+    }
     if (!b->use_graph) {
         RC_CK(cudaEventRecord(b->e0, b->st));
-        rc = b->dbl ? batch_enqueue<double>(b) : batch_enqueue<float>(b);
+        rc = b->dbl ? batch_enqueue<double>(b, false) : batch_enqueue<float>(b, false);
         if (rc) return rc;
         RC_CK(cudaEventRecord(b->e1, b->st));
         return RC_OK;
@@ -559,7 +651,7 @@ int rc_batch_run(rc_batch *b) {
             b->graph = nullptr;
         }
         RC_CK(cudaStreamBeginCapture(b->st, cudaStreamCaptureModeThreadLocal));
-        rc = b->dbl ? batch_enqueue<double>(b) : batch_enqueue<float>(b);
+        rc = b->dbl ? batch_enqueue<double>(b, true) : batch_enqueue<float>(b, true);
         cudaGraph_t g = nullptr;
         cudaError_t e = cudaStreamEndCapture(b->st, &g);
         if (rc) {
@@ -587,6 +679,17 @@ int rc_batch_wait(rc_batch *b, float *ms_device) {
     return RC_OK;
 }
 
+int rc_batch_phases(rc_batch *b, float *ms_setup, float *ms_march, float *ms_tally) {
+    if (!b) return set_err(nullptr, RC_E_INVALID, "NULL batch");
+    cudaSetDevice(b->device);
+    std::string *err_ = &b->err;
+    RC_CK(cudaEventSynchronize(b->e1));
+    if (ms_setup) RC_CK(cudaEventElapsedTime(ms_setup, b->e0, b->e_setup));
+    if (ms_march) RC_CK(cudaEventElapsedTime(ms_march, b->e_setup, b->e_march));
+    if (ms_tally) RC_CK(cudaEventElapsedTime(ms_tally, b->e_march, b->e1));
+    return RC_OK;
+}
+
 int rc_batch_collect(rc_batch *b, int index, float *Q, float *sigma, double *q64, double *var64, double *qw64,
                      double *vw64) {
     if (!b || index < 0 || index >= (int)b->m.size())
@@ -597,6 +700,16 @@ int rc_batch_collect(rc_batch *b, int index, float *Q, float *sigma, double *q64
     rc_ctx *c = b->m[index].ctx;
     void *slot = b->m[index].slot;
     int rc;
+    if (!q64 && !var64 && !qw64 && !vw64 && b->h_pack) {
+        // float results only: from the copy every run makes of all members
+        const float *pk = b->h_pack + b->pack_off[index];
+        if (c->dbl) rc = static_cast<Impl<double> *>(c->impl)->collect_packed(*static_cast<Slot<double> *>(slot), pk,
+                                                                             Q, sigma);
+        else rc = static_cast<Impl<float> *>(c->impl)->collect_packed(*static_cast<Slot<float> *>(slot), pk, Q,
+                                                                     sigma);
+        if (rc) return set_err(&b->err, rc, c->err);
+        return RC_OK;
+    }
     if (c->dbl)
         rc = static_cast<Impl<double> *>(c->impl)->copy_out(*static_cast<Slot<double> *>(slot), Q, sigma, q64, var64,
                                                              qw64, vw64);
@@ -622,8 +735,22 @@ int rc_batch_destroy(rc_batch *b) {
     if (b->d_outs) cudaFree(b->d_outs);
     if (b->h_outs) cudaFreeHost(b->h_outs);
     if (b->d_counter) cudaFree(b->d_counter);
+    if (b->d_segs) cudaFree(b->d_segs);
+    if (b->h_segs) cudaFreeHost(b->h_segs);
+    if (b->d_pack) cudaFree(b->d_pack);
+    if (b->h_pack) cudaFreeHost(b->h_pack);
     if (b->e0) cudaEventDestroy(b->e0);
     if (b->e1) cudaEventDestroy(b->e1);
+    if (b->e_setup) cudaEventDestroy(b->e_setup);
+    if (b->e_march) cudaEventDestroy(b->e_march);
+    if (b->fork) cudaEventDestroy(b->fork);
+    for (int k = 0; k < rc_batch::kSideStreams; ++k) {
+        if (b->side[k]) {
+            cudaStreamSynchronize(b->side[k]);
+            cudaStreamDestroy(b->side[k]);
+        }
+        if (b->join[k]) cudaEventDestroy(b->join[k]);
+    }
     if (b->st) cudaStreamDestroy(b->st);
     delete b;
     return RC_OK;

@@ -139,3 +139,42 @@ def test_request_arriving_during_a_long_solve_finishes_first():
     assert rb.t_submit > ra.t_admit          # it arrived while the long solve ran
     assert rb.latency < 0.25 * ra.latency
     srv.close()
+
+
+def test_serving_class_grid_tolerance_request_in_a_mix_equals_alone():
+    """A narrow-band request of a serving-mix size class (104x72x72, 100
+    bands x 8 g, 2% tolerance: the server picks photmax from a pilot) solved
+    while smaller requests arrive and run alongside it equals the same solve
+    alone at the photmax the server chose, bit for bit; so do the small
+    requests."""
+    tabs = W.tables_nb(nB=100, nQ=8, nT=64)
+    p = W.channel_params(104, 72, 72, photmax=64, nVar=4, levels=[(104, 72, 72), (52, 36, 36), (26, 18, 18)],
+                         maxs=[5, 5, 100000], calcwalls=1, adiabw=1)
+    p.seed = 4242
+    T = W.channel_field(p, seed=31)
+    small = []
+    for s in range(4):
+        q = W.channel_params(32, 32, 32, photmax=32 * (s + 1), nVar=4, levels=[(32, 32, 32), (16, 16, 16)],
+                             maxs=[5, 100000])
+        q.seed = 500 + s
+        small.append((q, W.channel_field(q, seed=40 + s)))
+    srv = api.Server(max_inflight=8)
+    ts = srv.add_tables(tabs)
+    big = srv.submit(p, T, table_set=ts, tolerance=0.02)
+    ids = [srv.submit(q, Tq, table_set=ts) for q, Tq in small]
+    rb = srv.wait(big)
+    rs = [srv.wait(i) for i in ids]
+    srv.close()
+    assert rb.photmax > 64 and rb.rel_std_maxq < 1.3 * 0.02
+    pa = api.copy_params(p)
+    pa.photmax = rb.photmax
+    s = api.Solver(pa, tabs)
+    alone = s.solve(T, want64=False)
+    s.close()
+    np.testing.assert_array_equal(rb.Q, alone.Q)
+    np.testing.assert_array_equal(rb.sigma, alone.sigma)
+    for (q, Tq), r in zip(small, rs):
+        s = api.Solver(q, tabs)
+        a = s.solve(Tq, want64=False)
+        s.close()
+        np.testing.assert_array_equal(r.Q, a.Q)
