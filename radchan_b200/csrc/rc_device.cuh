@@ -537,13 +537,14 @@ __device__ __forceinline__ void absorb(Ray<R> &r, R ds, R absco, R blackpow) {
 // continuous OERM tally, so the emission-based reciprocity weights are
 // unchanged (the exchange between two cells is reciprocal for a phase
 // function of the scattering angle alone).
+// What a step needs of a scattering bundle; the counter words and the event
+// count (needed only at an event) are kept apart, in shared memory in the
+// march, so the step loop carries two registers more, not six.
 template <typename R>
 struct ScatState {
-    uint32_t cx, cy, cz;  // Philox counter words of the bundle
-    int nev;              // scattering events so far
-    R ks;                 // scattering coefficient of the bundle's band and g point
-    R tau;                // optical depth left to the next event
-    bool turn;            // stopped at an event, new direction not drawn yet
+    R ks;   // scattering coefficient of the bundle's band and g point
+    R tau;  // optical depth left to the next event; < 0: stopped at an event,
+            // new direction not drawn yet
 };
 
 // A ring entry of a scattering medium: the emitted bundle, its counter
@@ -576,21 +577,22 @@ __device__ __forceinline__ void scatter_start(uint32_t &cx, uint32_t &cy, uint32
     }
 }
 
-// New direction at scattering event q.nev + 1 of a bundle in band nb, and
-// the optical depth to the event after it.  The direction is turned by the
+// New direction at the next scattering event of a bundle in band r.nb (ctr:
+// its counter words x, y, z and the number of events so far in w), and the
+// optical depth to the event after it.  The direction is turned by the
 // sampled polar angle theta about the old one, with azimuth phi measured
 // from the plane of the old direction and the z axis (the standard rotation
 // of Monte Carlo transport codes; near |s_z| = 1 the new direction is taken
 // about the z axis itself).  Zero components are floored to 1e-10 as at
 // emission (:132-137).
 template <typename R>
-__device__ __noinline__ void scatter_turn(Ray<R> &r, ScatState<R> &q, const DSolve<R> &S) {
-    q.nev += 1;
+__device__ __noinline__ void scatter_turn(Ray<R> &r, uint4 &ctr, ScatState<R> &q, const DSolve<R> &S) {
+    ctr.w += 1u;
     rc_u32x4 c;
-    c.x = q.cx;
-    c.y = q.cy;
-    c.z = q.cz;
-    c.w = (uint32_t)(q.nev + 1);
+    c.x = ctr.x;
+    c.y = ctr.y;
+    c.z = ctr.z;
+    c.w = ctr.w + 1u;
     const rc_u32x4 d = rc_philox4x32_10(c, S.key0, S.key1);
     const R u_t = (R)rc_u01(d.x), u_p = (R)rc_u01(d.y), u_s = (R)rc_u01(d.z);
     const int nA = S.nA;
@@ -633,15 +635,13 @@ __device__ __noinline__ void scatter_turn(Ray<R> &r, ScatState<R> &q, const DSol
     q.tau = -RT<R>::log_(u_s);
 }
 
-// Scattering state of a bundle taken from the ring.
+// Scattering state of a bundle taken from the ring (ctr: its counter words,
+// no event yet).
 template <typename R>
-__device__ __forceinline__ void place_scatter(ScatState<R> &q, const DSolve<R> &S, const EmittedScat<R> &e) {
-    q.cx = e.cx;
-    q.cy = e.cy;
-    q.cz = e.cz;
+__device__ __forceinline__ void place_scatter(ScatState<R> &q, uint4 &ctr, const DSolve<R> &S,
+                                              const EmittedScat<R> &e) {
+    ctr = make_uint4(e.cx, e.cy, e.cz, 0u);
     q.tau = e.tau;
-    q.nev = 0;
-    q.turn = false;
     const int nb = e.e.nbg & 0xfffff, g = e.e.nbg >> 20;
     q.ks = (S.nA > 0) ? S.ksca[RC_IX((size_t)nb * S.nQ + g, (long long)S.nB * S.nQ, SITE_KSCA, S)] : (R)0;
 }
@@ -663,7 +663,7 @@ __device__ __forceinline__ const Emitted<R> &entry_base(const EmittedScat<R> &e)
 // direction component (never 0: emission floors it at 1e-10).  With SCAT, a
 // bundle whose scattering optical depth over the step exceeds what is left
 // to its next event stops at the event inside the cell (absorbing along
-// the shortened path), counts the event as a step and sets qs.turn: the
+// the shortened path), counts the event as a step and sets qs.tau < 0: the
 // caller draws the new direction (scatter_turn) before the next step.  The
 // turn depends neither on the cell nor on the level, so a caller may
 // advance the level first and gather the turns of several lanes into one
@@ -702,7 +702,7 @@ __device__ __forceinline__ int march_step(Ray<R> &r, ScatState<R> &qs, const DSo
             r.yp = RT<R>::fma_(dsc, r.sy, r.yp);
             r.zp = RT<R>::fma_(dsc, r.sz, r.zp);
             absorb(r, dsc, absco, blackpow);
-            qs.turn = true;
+            qs.tau = (R)-1;
             r.counter += 1;
             return B.w;
         }

@@ -326,8 +326,9 @@ __global__ void k_trace(const DSolve<R> *Sp, int n, const rc_bundle_id *ids, rc_
     if (ok) {
         Ray<R> r;
         ScatState<R> qs;
+        uint4 ctr;
         place_bundle(r, S, e);
-        if (SCAT) place_scatter(qs, S, es);
+        if (SCAT) place_scatter(qs, ctr, S, es);
         bool active = level_advance(r, S);
         int ns = 0;
         while (active) {
@@ -339,10 +340,7 @@ __global__ void k_trace(const DSolve<R> *Sp, int n, const rc_bundle_id *ids, rc_
                 c[3] = r.kc;
             }
             march_step<R, SCAT>(r, qs, S);
-            if (SCAT && qs.turn) {
-                scatter_turn(r, qs, S);
-                qs.turn = false;
-            }
+            if (SCAT && qs.tau < (R)0) scatter_turn(r, ctr, qs, S);
             ns++;
             active = r.tra > r.tol;
             if (active) active = level_advance(r, S);

@@ -120,9 +120,16 @@ __global__ void k_prio_tiles(const DSolve<R> *Sp, float thr, const float *kmin, 
     }
 }
 
-template <typename E>
+template <typename E, bool SCAT>
 struct WarpShared {
     E ring[kRing];
+};
+// with scattering, also the counter words and event count of every lane's
+// bundle (read and written by that lane only, at placement and at events)
+template <typename E>
+struct WarpShared<E, true> {
+    E ring[kRing];
+    uint4 ctr[kWarp];
 };
 
 // Ring entry of the march: the emitted bundle, plus its counter words and
@@ -163,8 +170,8 @@ __global__ void __launch_bounds__(256, MINB) k_march(MarchArgs a) {
     using Entry = RingEntry<R, SCAT>;
     extern __shared__ __align__(16) unsigned char smem[];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
-    WarpShared<Entry> *ws = reinterpret_cast<WarpShared<Entry> *>(smem) + warp;
-    const size_t wbytes = ((sizeof(WarpShared<Entry>) * nwarps) + 15) & ~(size_t)15;
+    WarpShared<Entry, SCAT> *ws = reinterpret_cast<WarpShared<Entry, SCAT> *>(smem) + warp;
+    const size_t wbytes = ((sizeof(WarpShared<Entry, SCAT>) * nwarps) + 15) & ~(size_t)15;
     const int pool_max = kWarp * a.rpt_max;
     double *slots0 = reinterpret_cast<double *>(smem + wbytes) + (size_t)warp * 2 * pool_max;
     const DSolve<R> *solves = reinterpret_cast<const DSolve<R> *>(a.solves);
@@ -332,7 +339,11 @@ __global__ void __launch_bounds__(256, MINB) k_march(MarchArgs a) {
                     const Entry &ee = ws->ring[(head + rank) & (kRing - 1)];
                     const Emitted<R> &e = entry_base(ee);
                     place_bundle(r, S, e);
-                    if constexpr (SCAT) place_scatter(qs, S, ee);
+                    if constexpr (SCAT) {
+                        uint4 c;
+                        place_scatter(qs, c, S, ee);
+                        ws->ctr[lane] = c;
+                    }
                     myb = (e.kk >> 18) & 0x7ff;
                     mypar = (e.kk >> 29) & 1;
                     took = true;
@@ -366,7 +377,7 @@ __global__ void __launch_bounds__(256, MINB) k_march(MarchArgs a) {
             for (;;) {
                 bool fin = false;
                 bool wait_turn = false;
-                if constexpr (SCAT) wait_turn = active && qs.turn;
+                if constexpr (SCAT) wait_turn = active && qs.tau < (R)0;
                 if (active && !wait_turn) {
                     const int budget = march_step<R, SCAT>(r, qs, S);
                     nsteps++;
@@ -376,9 +387,8 @@ __global__ void __launch_bounds__(256, MINB) k_march(MarchArgs a) {
                         slots0[mypar * pool_max + myb] = r.De;
                         active = false;
                         fin = true;
-                        if constexpr (SCAT) qs.turn = false;
                     }
-                    if constexpr (SCAT) wait_turn = active && qs.turn;
+                    if constexpr (SCAT) wait_turn = active && qs.tau < (R)0;
                 }
                 const unsigned fm = __ballot_sync(0xffffffffu, fin);
                 if (fm) {
@@ -399,9 +409,10 @@ __global__ void __launch_bounds__(256, MINB) k_march(MarchArgs a) {
         }
         // ---- scattering: the new directions of every lane stopped at an event
         if constexpr (SCAT) {
-            if (active && qs.turn) {
-                scatter_turn(r, qs, S);
-                qs.turn = false;
+            if (active && qs.tau < (R)0) {
+                uint4 c = ws->ctr[lane];
+                scatter_turn(r, c, qs, S);
+                ws->ctr[lane].w = c.w;
             }
         }
         // ---- reduce finished tiles: chunk sums in bundle order, group sums
@@ -432,7 +443,7 @@ __global__ void __launch_bounds__(256, MINB) k_march(MarchArgs a) {
 
 template <typename R, bool SCAT>
 constexpr size_t march_smem_bytes(int block, int rpt_max) {
-    return ((((size_t)sizeof(WarpShared<RingEntry<R, SCAT>>) * (block / kWarp)) + 15) & ~(size_t)15) +
+    return ((((size_t)sizeof(WarpShared<RingEntry<R, SCAT>, SCAT>) * (block / kWarp)) + 15) & ~(size_t)15) +
            (size_t)(block / kWarp) * 2 * kWarp * rpt_max * sizeof(double);
 }
 

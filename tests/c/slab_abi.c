@@ -39,10 +39,15 @@ int main(int argc, char **argv) {
         fprintf(stderr, "slab_abi: param.h must set p_col > 1 dividing kmax\n");
         return 2;
     }
+    /* tables in the reference's file formats; both solves read them back
+     * from the files (the text format rounds the synthetic values) */
     rc_synth_spec spec = {p.nB, p.nQ, p.nT, 300.0, 2000.0, 500.0, 10000.0, -3.0, 2.0, 1.0, 1.5, 20240601u};
     rc_table_set *ts = NULL;
     if (rc_tables_synthetic(&spec, &ts)) return fail("rc_tables_synthetic");
     if (rc_tables_write_dir(ts, argv[3])) return fail("rc_tables_write_dir");
+    rc_tables_free(ts);
+    ts = NULL;
+    if (rc_tables_read_dir(argv[3], p.nT, p.nB, p.nQ, &ts)) return fail("rc_tables_read_dir");
 
     const int ni = p.imax + 2, nj = p.jmax + 2, nk = p.kmax + 2;
     float *T = (float *)malloc((size_t)ni * nj * nk * sizeof(float));
