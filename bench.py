@@ -82,6 +82,10 @@ def workload_desc(name, p):
     if name == "grey32":
         return dict(workload="grey OERM kappa=1, 32^3 channel, photmax %d, nVar 4" % p.photmax, grid=[32, 32, 32],
                     photmax=p.photmax, nVar=4, levels=1)
+    if name == "c4":
+        return dict(workload="narrow-band 100x8 OERM, optically thick, 192x128x128 channel, specular y, "
+                             "photmax %d, nVar %d" % (p.photmax, p.nVar), grid=[192, 128, 128], bands=100, gpoints=8,
+                    temps=64, photmax=p.photmax, nVar=p.nVar, levels=p.grid_num)
     raise SystemExit("unknown workload " + name)
 
 
@@ -99,6 +103,12 @@ def workload(name, photmax=0):
     elif name == "grey32":
         p = W.config_grey_32(photmax=photmax or 64)
         tabs = None
+    elif name == "c4":
+        # the precision study's channel (192x128x128, optically thick tables,
+        # emissivity 0.8, specular y walls): profiling runs of the march on a
+        # 3.1 M-cell pyramid
+        p = W.config_precision(photmax=photmax or 1024)
+        tabs = W.tables_nb(logk_lo=-1.0, logk_hi=2.0)
     else:
         raise SystemExit("unknown workload " + name)
     return p, tabs, W.channel_field(p), workload_desc(name, p)
@@ -365,6 +375,45 @@ def leg_at_tolerance(p, tabs, T, rel0, dev, flush, tol=0.01, steps=2):
     sec = sum(ms) / 1000.0
     return {"tolerance": tol, "photmax": q.photmax, "rel_std_maxq": rel, "ms_per_solve": 1000 * sec / steps,
             "solves_per_s": steps / sec, "bundles_per_s": bundles / sec, "steps": steps}
+
+
+def leg_scattering(p, tabs, T, dev, flush, steps=3):
+    """The benchmark solve with particle scattering added (synthetic
+    Henyey-Greenstein tables: scattering coefficient log-uniform on
+    [0.1, 1] per band, asymmetry g uniform on [0, 0.8], 181 angles): device
+    time, bundles/s, ray-cell steps/s (scattering events count as steps)
+    next to the same solve without particles."""
+    import torch
+
+    from radchan_b200 import api
+    s = api.Solver(p, tabs, device=dev)
+    T_dev = torch.from_numpy(T).to(f"cuda:{dev}")
+
+    def timed():
+        t = s.solve_device_async(T_dev.data_ptr())
+        s.wait_device(t)
+        s.release(t)
+        ms, bundles, nsteps = [], 0.0, 0.0
+        for _ in range(steps):
+            flush.zero_()
+            torch.cuda.synchronize()
+            t = s.solve_device_async(T_dev.data_ptr())
+            info = s.info(t)
+            ms.append(info.ms_solve)
+            bundles += info.bundles
+            nsteps += info.steps
+            s.release(t)
+        sec = sum(ms) / 1000.0
+        return {"ms_per_solve": 1000 * sec / steps, "bundles_per_s": bundles / sec, "steps_per_s": nsteps / sec,
+                "steps_per_bundle": nsteps / bundles}
+
+    plain = timed()
+    sc = api.Scattering.synthetic(nB=p.nB, nQ=p.nQ, nA=181, ksca_lo=0.1, ksca_hi=1.0, g_lo=0.0, g_hi=0.8, seed=3)
+    s.set_scattering(sc)
+    scat = timed()
+    s.close()
+    return {"particles": "ksca log-uniform [0.1, 1] 1/m per band, Henyey-Greenstein g ~ U[0, 0.8], 181 angles",
+            "with_scattering": scat, "without": plain}
 
 
 def leg_dns_source(dev, flush, reps=20, cpu=True):
@@ -839,6 +888,8 @@ def run_ours(args, ws, rank, local):
         # 32/128), where one solve does not fill the GPU
         line["batched_small"] = leg_batched(dev, edges=(16, 24, 32), photmaxes=(32, 128))
         line["dns_source"] = leg_dns_source(dev, flush, cpu=not args.no_cpu_baseline)
+        # the same solve in a medium with scattering particles
+        line["scattering"] = leg_scattering(p, tabs, T, dev, flush)
         # the same mixes at equal 1% relative std of max|Q| (photmax per
         # problem from a pilot), one pass each
         line["batched_at_1pct"] = leg_batched(dev, passes=1, tol=0.01, served=False, warm=False)

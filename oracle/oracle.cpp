@@ -152,11 +152,11 @@ int g_ref_wall_edge = 0;
 // Particle scattering tables of later solves (oracle_set_scattering), raw
 // as the caller gave them: no scattering while nA == 0.  The march
 // restates the device's scattering step (rc_device.cuh scatter_start,
-// scatter_turn, march_step with SCAT): free path -ln(u) against the
-// scattering coefficient, polar angle from the band's phase CDF (linear in
-// angle between table angles), uniform azimuth, the standard rotation about
-// the old direction; draws from the bundle's Philox counter with the event
-// number in the fourth word.
+// scatter_turn, march_step with SCAT): free path -ln(u) / k_s (none when
+// k_s = 0), polar angle from the band's phase CDF (linear in angle between
+// table angles), uniform azimuth, the standard rotation about the old
+// direction; draws from the bundle's Philox counter with the event number in
+// the fourth word.
 struct ScatTables {
     int nB = 0, nQ = 0, nA = 0;
     std::vector<float> ksca, theta, cdf;
@@ -437,10 +437,11 @@ struct Problem {
         R xp, yp, zp, sx, sy, sz, isx, isy, isz, tra;
         int flag[3];
         // scattering: counter words of the bundle, events so far, the
-        // scattering coefficient of its band and g point, optical depth left
+        // scattering coefficient of its band and g point, distance left to
+        // the next event
         uint32_t cx, cy, cz;
         int nev;
-        R ks, tau;
+        R ks, dist;
     };
 
     // Absorption along ds (mc_gpu_noint.cu:358-370).
@@ -508,7 +509,7 @@ struct Problem {
         ray.flag[0] = ray.sx < 0;
         ray.flag[1] = ray.sy < 0;
         ray.flag[2] = ray.sz < 0;
-        ray.tau = -M<R>::log_(u_s);
+        ray.dist = -M<R>::log_(u_s) / ray.ks;
     }
 
     R Tcell(int lev, int ic, int jc, int kc) const {
@@ -602,11 +603,9 @@ struct Problem {
             if (ds > dsy) ds = dsy;
             if (ds > dsz) ds = dsz;
             if (nA > 0) {
-                R dts = ds * ray.ks;
-                if (dts > ray.tau) {
+                if (ds > ray.dist) {
                     // the next scattering event lies inside this cell
-                    R dsc = ray.tau / ray.ks;
-                    if (dsc > ds) dsc = ds;
+                    R dsc = ray.dist;
                     ray.xp = M<R>::fma_(dsc, ray.sx, ray.xp);
                     ray.yp = M<R>::fma_(dsc, ray.sy, ray.yp);
                     ray.zp = M<R>::fma_(dsc, ray.sz, ray.zp);
@@ -615,7 +614,7 @@ struct Problem {
                     counter += 1;
                     continue;
                 }
-                ray.tau = ray.tau - dts;
+                ray.dist = ray.dist - ds;
             }
             if (ds == dsx) ray.xp = fxu;
             else ray.xp = M<R>::fma_(ds, ray.sx, ray.xp);
@@ -730,13 +729,12 @@ struct Problem {
         ray.cy = ctr.y;
         ray.cz = ctr.z;
         ray.nev = 0;
-        ray.ks = 0;
-        ray.tau = (R)3.0e38f;
-        if (nA > 0) {
+        ray.ks = (nA > 0) ? ksca[(size_t)nb * nQ + g] : (R)0;
+        ray.dist = (R)3.0e38f;
+        if (ray.ks > (R)0) {
             rc_u32x4 c1 = {ctr.x, ctr.y, ctr.z, 1u};
             rc_u32x4 d1 = rc_philox4x32_10(c1, (uint32_t)p.seed, (uint32_t)(p.seed >> 32));
-            ray.tau = -M<R>::log_((R)rc_u01(d1.x));
-            ray.ks = ksca[(size_t)nb * nQ + g];
+            ray.dist = -M<R>::log_((R)rc_u01(d1.x)) / ray.ks;
         }
         if (rec) {
             rec->nb = nb;

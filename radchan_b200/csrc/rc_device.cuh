@@ -529,64 +529,67 @@ __device__ __forceinline__ void absorb(Ray<R> &r, R ds, R absco, R blackpow) {
 // of a scattering medium carries, besides its Ray, the Philox counter words
 // of its emission (h, v | kind << 24, cell): draw n (the fourth counter word
 // n >= 1; emission uses 0) is its n-th draw after emission.  Draw 1 gives
-// the optical depth to the first scattering event, tau = -ln(u); at event n
-// draw n+1 gives the scattering angle (the band's cumulative phase
-// probability inverted, linear in angle between table angles), the azimuth
-// (uniform) and the optical depth to the next event.  The free path is
+// the free path to the first scattering event, -ln(u) / k_s with k_s the
+// scattering coefficient of its band and g point (no event when k_s = 0);
+// at event n draw n+1 gives the scattering angle (the band's cumulative
+// phase probability inverted, linear in angle between table angles), the
+// azimuth (uniform) and the free path to the next event.  The free path is
 // sampled against the scattering coefficient alone; absorption stays the
 // continuous OERM tally, so the emission-based reciprocity weights are
 // unchanged (the exchange between two cells is reciprocal for a phase
 // function of the scattering angle alone).
-// What a step needs of a scattering bundle; the counter words and the event
-// count (needed only at an event) are kept apart, in shared memory in the
-// march, so the step loop carries two registers more, not six.
+// What a step needs of a scattering bundle is one register: the distance
+// left to its next event.  The counter words, event count and k_s (needed
+// only at an event) are kept apart, in shared memory in the march.
+constexpr float kNoEvent = 3.0e38f;  // free path of a bundle whose band does not scatter
 template <typename R>
 struct ScatState {
-    R ks;   // scattering coefficient of the bundle's band and g point
-    R tau;  // optical depth left to the next event; < 0: stopped at an event,
-            // new direction not drawn yet
+    R dist;  // distance left to the next event; < 0: stopped at an event,
+             // new direction not drawn yet
 };
 
-// A ring entry of a scattering medium: the emitted bundle, its counter
-// words and the optical depth to its first event.
+// Scattering coefficient of band nb, g point g (0 without particles).
 template <typename R>
-struct alignas(16) EmittedScat {
-    Emitted<R> e;
-    uint32_t cx, cy, cz;
-    R tau;
-};
+__device__ __forceinline__ R scatter_coef(const DSolve<R> &S, int nb, int g) {
+    return (S.nA > 0) ? S.ksca[RC_IX((size_t)nb * S.nQ + g, (long long)S.nB * S.nQ, SITE_KSCA, S)] : (R)0;
+}
 
-// The counter words and first free path of an emitted bundle (draw 1).
+// Philox counter words of a bundle (emission's: h, v | kind << 24, cell),
+// with the event count in w.
+__device__ __forceinline__ uint4 scatter_counter(uint32_t imax, uint32_t jmax, int kind, int i, int j, int k, int v,
+                                                 int h, uint32_t nev) {
+    const uint32_t cell = (kind == 0) ? (uint32_t)((i - 1) + imax * ((j - 1) + jmax * (k - 1)))
+                                      : (uint32_t)((j - 1) + jmax * (k - 1));
+    return make_uint4((uint32_t)h, (uint32_t)v | ((uint32_t)kind << 24), cell, nev);
+}
+
+// Free path to the first event of a bundle with counter words ctr and
+// scattering coefficient ks (draw 1; kNoEvent when ks = 0).
 template <typename R>
-__device__ __forceinline__ void scatter_start(uint32_t &cx, uint32_t &cy, uint32_t &cz, R &tau, const DSolve<R> &S,
-                                              int kind, int i, int j, int k, int v, int h) {
-    cx = (uint32_t)h;
-    cy = (uint32_t)v | ((uint32_t)kind << 24);
-    cz = (kind == 0) ? (uint32_t)((i - 1) + S.imax * ((j - 1) + S.jmax * (k - 1)))
-                     : (uint32_t)((j - 1) + S.jmax * (k - 1));
-    if (S.nA > 0) {
+__device__ __forceinline__ R scatter_first_dist(const DSolve<R> &S, uint4 ctr, R ks) {
+    R dist = (R)kNoEvent;
+    if (ks > (R)0) {
         rc_u32x4 c;
-        c.x = cx;
-        c.y = cy;
-        c.z = cz;
+        c.x = ctr.x;
+        c.y = ctr.y;
+        c.z = ctr.z;
         c.w = 1u;
         const rc_u32x4 d = rc_philox4x32_10(c, S.key0, S.key1);
-        tau = -RT<R>::log_((R)rc_u01(d.x));
-    } else {
-        tau = (R)3.0e38f;
+        dist = -RT<R>::log_((R)rc_u01(d.x)) / ks;
     }
+    return dist;
 }
 
 // New direction at the next scattering event of a bundle in band r.nb (ctr:
-// its counter words x, y, z and the number of events so far in w), and the
-// optical depth to the event after it.  The direction is turned by the
+// its counter words x, y, z and the number of events so far in w; ks > 0 its
+// scattering coefficient), and the free path to the event after it.  The direction is turned by the
 // sampled polar angle theta about the old one, with azimuth phi measured
 // from the plane of the old direction and the z axis (the standard rotation
 // of Monte Carlo transport codes; near |s_z| = 1 the new direction is taken
 // about the z axis itself).  Zero components are floored to 1e-10 as at
 // emission (:132-137).
 template <typename R>
-__device__ __noinline__ void scatter_turn(Ray<R> &r, uint4 &ctr, ScatState<R> &q, const DSolve<R> &S) {
+__device__ __noinline__ void scatter_turn(Ray<R> &r, uint4 &ctr, R ks, ScatState<R> &q, const DSolve<R> &S) {
     ctr.w += 1u;
     rc_u32x4 c;
     c.x = ctr.x;
@@ -632,39 +635,18 @@ __device__ __noinline__ void scatter_turn(Ray<R> &r, uint4 &ctr, ScatState<R> &q
     r.isx = (R)1 / nx;
     r.isy = (R)1 / ny;
     r.isz = (R)1 / nz;
-    q.tau = -RT<R>::log_(u_s);
+    q.dist = -RT<R>::log_(u_s) / ks;
 }
-
-// Scattering state of a bundle taken from the ring (ctr: its counter words,
-// no event yet).
-template <typename R>
-__device__ __forceinline__ void place_scatter(ScatState<R> &q, uint4 &ctr, const DSolve<R> &S,
-                                              const EmittedScat<R> &e) {
-    ctr = make_uint4(e.cx, e.cy, e.cz, 0u);
-    q.tau = e.tau;
-    const int nb = e.e.nbg & 0xfffff, g = e.e.nbg >> 20;
-    q.ks = (S.nA > 0) ? S.ksca[RC_IX((size_t)nb * S.nQ + g, (long long)S.nB * S.nQ, SITE_KSCA, S)] : (R)0;
-}
-
-// The emitted bundle inside a ring entry of either kind.
-template <typename R>
-__device__ __forceinline__ Emitted<R> &entry_base(Emitted<R> &e) { return e; }
-template <typename R>
-__device__ __forceinline__ Emitted<R> &entry_base(EmittedScat<R> &e) { return e.e; }
-template <typename R>
-__device__ __forceinline__ const Emitted<R> &entry_base(const Emitted<R> &e) { return e; }
-template <typename R>
-__device__ __forceinline__ const Emitted<R> &entry_base(const EmittedScat<R> &e) { return e.e; }
 
 // One ray-cell crossing (one iteration of the while loop of march_ray,
 // :252-656).  Returns the step budget (maxs) of the level the step was
 // taken on, which the caller compares with the step counter.  The side of
 // the cell a ray leaves through on each axis follows from the sign of its
 // direction component (never 0: emission floors it at 1e-10).  With SCAT, a
-// bundle whose scattering optical depth over the step exceeds what is left
-// to its next event stops at the event inside the cell (absorbing along
-// the shortened path), counts the event as a step and sets qs.tau < 0: the
-// caller draws the new direction (scatter_turn) before the next step.  The
+// bundle whose step is longer than the distance left to its next event
+// stops at the event inside the cell (absorbing along the shortened path),
+// counts the event as a step and sets qs.dist < 0: the caller draws the new
+// direction (scatter_turn) before the next step.  The
 // turn depends neither on the cell nor on the level, so a caller may
 // advance the level first and gather the turns of several lanes into one
 // pass.
@@ -693,20 +675,18 @@ __device__ __forceinline__ int march_step(Ray<R> &r, ScatState<R> &qs, const DSo
     if (ds > dsy) ds = dsy;
     if (ds > dsz) ds = dsz;
     if constexpr (SCAT) {
-        const R dts = ds * qs.ks;
-        if (dts > qs.tau) {
+        if (ds > qs.dist) {
             // the next scattering event lies inside this cell
-            R dsc = qs.tau / qs.ks;
-            if (dsc > ds) dsc = ds;
+            const R dsc = qs.dist;
             r.xp = RT<R>::fma_(dsc, r.sx, r.xp);
             r.yp = RT<R>::fma_(dsc, r.sy, r.yp);
             r.zp = RT<R>::fma_(dsc, r.sz, r.zp);
             absorb(r, dsc, absco, blackpow);
-            qs.tau = (R)-1;
+            qs.dist = (R)-1;
             r.counter += 1;
             return B.w;
         }
-        qs.tau = qs.tau - dts;
+        qs.dist = qs.dist - ds;
     }
     r.xp = (ds == dsx) ? fxu : RT<R>::fma_(ds, r.sx, r.xp);
     r.yp = (ds == dsy) ? fyu : RT<R>::fma_(ds, r.sy, r.yp);

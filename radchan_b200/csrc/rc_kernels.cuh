@@ -314,10 +314,8 @@ __global__ void k_trace(const DSolve<R> *Sp, int n, const rc_bundle_id *ids, rc_
     rec.sx = rec.sy = rec.sz = 0.f;
     rec.tra = 0.f;
     rec.De = 0.0;
-    EmittedScat<R> es;
-    Emitted<R> &e = es.e;
+    Emitted<R> e;
     const bool ok = emit_bundle(e, S, id.kind, id.i, id.j, id.k, id.v, id.h);
-    if (SCAT) scatter_start(es.cx, es.cy, es.cz, es.tau, S, id.kind, id.i, id.j, id.k, id.v, id.h);
     rec.nb = e.nbg & 0xfffff;
     rec.g = e.nbg >> 20;
     rec.sx = (float)e.sx;
@@ -326,9 +324,14 @@ __global__ void k_trace(const DSolve<R> *Sp, int n, const rc_bundle_id *ids, rc_
     if (ok) {
         Ray<R> r;
         ScatState<R> qs;
-        uint4 ctr;
+        uint4 ctr = make_uint4(0u, 0u, 0u, 0u);
+        R ks = (R)0;
         place_bundle(r, S, e);
-        if (SCAT) place_scatter(qs, ctr, S, es);
+        if (SCAT) {
+            ctr = scatter_counter(S.imax, S.jmax, id.kind, id.i, id.j, id.k, id.v, id.h, 0u);
+            ks = scatter_coef(S, e.nbg & 0xfffff, e.nbg >> 20);
+            qs.dist = scatter_first_dist(S, ctr, ks);
+        }
         bool active = level_advance(r, S);
         int ns = 0;
         while (active) {
@@ -340,7 +343,7 @@ __global__ void k_trace(const DSolve<R> *Sp, int n, const rc_bundle_id *ids, rc_
                 c[3] = r.kc;
             }
             march_step<R, SCAT>(r, qs, S);
-            if (SCAT && qs.tau < (R)0) scatter_turn(r, ctr, qs, S);
+            if (SCAT && qs.dist < (R)0) scatter_turn(r, ctr, ks, qs, S);
             ns++;
             active = r.tra > r.tol;
             if (active) active = level_advance(r, S);

@@ -1,8 +1,6 @@
 // rc_march.cuh -- the persistent march kernel (kernel_fluid + march_ray +
 // kernel_surface of src/montecarlo/mc_gpu_noint.cu, restructured for SIMT).
 #pragma once
-#include <type_traits>
-
 #include "rc_device.cuh"
 
 namespace rc {
@@ -120,22 +118,22 @@ __global__ void k_prio_tiles(const DSolve<R> *Sp, float thr, const float *kmin, 
     }
 }
 
-template <typename E, bool SCAT>
-struct WarpShared {
-    E ring[kRing];
-};
-// with scattering, also the counter words and event count of every lane's
-// bundle (read and written by that lane only, at placement and at events)
-template <typename E>
-struct WarpShared<E, true> {
-    E ring[kRing];
-    uint4 ctr[kWarp];
-};
-
-// Ring entry of the march: the emitted bundle, plus its counter words and
-// first free path when the medium scatters.
 template <typename R, bool SCAT>
-using RingEntry = typename std::conditional<SCAT, EmittedScat<R>, Emitted<R>>::type;
+struct WarpShared {
+    Emitted<R> ring[kRing];
+};
+// With scattering, also the free path to the first event of every ring
+// entry (drawn by the emission wave), and the scattering coefficient and
+// event count of every lane's bundle (read and written by that lane only,
+// at placement and at events; its counter words are decoded again from its
+// work item at an event).  The ring entries keep their 32 bytes.
+template <typename R>
+struct WarpShared<R, true> {
+    Emitted<R> ring[kRing];
+    R dist[kRing];
+    R ks[kWarp];
+    uint32_t nev[kWarp];
+};
 
 // Index of the solve owning a global tile (tile_start is an exclusive prefix).
 __device__ __forceinline__ int solve_of_tile(const long long *tile_start, int nsolves, unsigned long long tile) {
@@ -167,11 +165,10 @@ __device__ __forceinline__ void flush_counters(DScalars *sc, unsigned long long 
 // media with scattering particles (solves without them run in it unchanged).
 template <typename R, int MINB, bool SCAT>
 __global__ void __launch_bounds__(256, MINB) k_march(MarchArgs a) {
-    using Entry = RingEntry<R, SCAT>;
     extern __shared__ __align__(16) unsigned char smem[];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
-    WarpShared<Entry, SCAT> *ws = reinterpret_cast<WarpShared<Entry, SCAT> *>(smem) + warp;
-    const size_t wbytes = ((sizeof(WarpShared<Entry, SCAT>) * nwarps) + 15) & ~(size_t)15;
+    WarpShared<R, SCAT> *ws = reinterpret_cast<WarpShared<R, SCAT> *>(smem) + warp;
+    const size_t wbytes = ((sizeof(WarpShared<R, SCAT>) * nwarps) + 15) & ~(size_t)15;
     const int pool_max = kWarp * a.rpt_max;
     double *slots0 = reinterpret_cast<double *>(smem + wbytes) + (size_t)warp * 2 * pool_max;
     const DSolve<R> *solves = reinterpret_cast<const DSolve<R> *>(a.solves);
@@ -285,8 +282,8 @@ __global__ void __launch_bounds__(256, MINB) k_march(MarchArgs a) {
         // ---- converged emission wave: one bundle per lane
         if (count < kWarp && epar >= 0 && !((emitted >> epar) & 1u)) {
             const int b = next_b + lane;
-            Entry ee;
-            Emitted<R> &e = entry_base(ee);
+            Emitted<R> e;
+            R dist0 = (R)kNoEvent;
             bool ok = false;
             if (b < pool) {
                 const ItemId it = decode_item(S, (epar ? item0_1 : item0_0) + (b >> lrpt));
@@ -295,7 +292,10 @@ __global__ void __launch_bounds__(256, MINB) k_march(MarchArgs a) {
                     nbund++;
                     ok = emit_bundle(e, S, it.kind, it.i, it.j, it.k, it.v, h);
                     e.kk |= (b << 18) | (epar << 29);
-                    if constexpr (SCAT) scatter_start(ee.cx, ee.cy, ee.cz, ee.tau, S, it.kind, it.i, it.j, it.k, it.v, h);
+                    if constexpr (SCAT)
+                        dist0 = scatter_first_dist(
+                            S, scatter_counter(S.imax, S.jmax, it.kind, it.i, it.j, it.k, it.v, h, 0u),
+                            scatter_coef(S, e.nbg & 0xfffff, e.nbg >> 20));
                 }
             }
             const unsigned m = __ballot_sync(0xffffffffu, ok);
@@ -320,7 +320,10 @@ __global__ void __launch_bounds__(256, MINB) k_march(MarchArgs a) {
                 }
                 pos = rank;
             }
-            if (ok) ws->ring[(head + count + pos) & (kRing - 1)] = ee;
+            if (ok) {
+                ws->ring[(head + count + pos) & (kRing - 1)] = e;
+                if constexpr (SCAT) ws->dist[(head + count + pos) & (kRing - 1)] = dist0;
+            }
             count += __popc(m);
             if (epar) out1 += __popc(m);
             else out0 += __popc(m);
@@ -336,13 +339,12 @@ __global__ void __launch_bounds__(256, MINB) k_march(MarchArgs a) {
             if (!active) {
                 const int rank = __popc(m & lt);
                 if (rank < navail) {
-                    const Entry &ee = ws->ring[(head + rank) & (kRing - 1)];
-                    const Emitted<R> &e = entry_base(ee);
+                    const Emitted<R> &e = ws->ring[(head + rank) & (kRing - 1)];
                     place_bundle(r, S, e);
                     if constexpr (SCAT) {
-                        uint4 c;
-                        place_scatter(qs, c, S, ee);
-                        ws->ctr[lane] = c;
+                        qs.dist = ws->dist[(head + rank) & (kRing - 1)];
+                        ws->ks[lane] = scatter_coef(S, e.nbg & 0xfffff, e.nbg >> 20);
+                        ws->nev[lane] = 0u;
                     }
                     myb = (e.kk >> 18) & 0x7ff;
                     mypar = (e.kk >> 29) & 1;
@@ -377,7 +379,7 @@ __global__ void __launch_bounds__(256, MINB) k_march(MarchArgs a) {
             for (;;) {
                 bool fin = false;
                 bool wait_turn = false;
-                if constexpr (SCAT) wait_turn = active && qs.tau < (R)0;
+                if constexpr (SCAT) wait_turn = active && qs.dist < (R)0;
                 if (active && !wait_turn) {
                     const int budget = march_step<R, SCAT>(r, qs, S);
                     nsteps++;
@@ -388,7 +390,7 @@ __global__ void __launch_bounds__(256, MINB) k_march(MarchArgs a) {
                         active = false;
                         fin = true;
                     }
-                    if constexpr (SCAT) wait_turn = active && qs.tau < (R)0;
+                    if constexpr (SCAT) wait_turn = active && qs.dist < (R)0;
                 }
                 const unsigned fm = __ballot_sync(0xffffffffu, fin);
                 if (fm) {
@@ -409,10 +411,12 @@ __global__ void __launch_bounds__(256, MINB) k_march(MarchArgs a) {
         }
         // ---- scattering: the new directions of every lane stopped at an event
         if constexpr (SCAT) {
-            if (active && qs.tau < (R)0) {
-                uint4 c = ws->ctr[lane];
-                scatter_turn(r, c, qs, S);
-                ws->ctr[lane].w = c.w;
+            if (active && qs.dist < (R)0) {
+                const ItemId it = decode_item(S, (mypar ? item0_1 : item0_0) + (myb >> lrpt));
+                uint4 c = scatter_counter(S.imax, S.jmax, it.kind, it.i, it.j, it.k, it.v, it.h0 + (myb & (rpt - 1)),
+                                          ws->nev[lane]);
+                scatter_turn(r, c, ws->ks[lane], qs, S);
+                ws->nev[lane] = c.w;
             }
         }
         // ---- reduce finished tiles: chunk sums in bundle order, group sums
@@ -443,7 +447,7 @@ __global__ void __launch_bounds__(256, MINB) k_march(MarchArgs a) {
 
 template <typename R, bool SCAT>
 constexpr size_t march_smem_bytes(int block, int rpt_max) {
-    return ((((size_t)sizeof(WarpShared<RingEntry<R, SCAT>, SCAT>) * (block / kWarp)) + 15) & ~(size_t)15) +
+    return ((((size_t)sizeof(WarpShared<R, SCAT>) * (block / kWarp)) + 15) & ~(size_t)15) +
            (size_t)(block / kWarp) * 2 * kWarp * rpt_max * sizeof(double);
 }
 
