@@ -154,16 +154,18 @@ struct ImplBase {
     virtual ~ImplBase() {}
 };
 
-// Gather of float result arrays into one buffer: segment blockIdx.y copies
-// n floats from src to dst + off (batch results, one copy to the host).
-struct PackSeg {
+// Many copies in one launch: segment blockIdx.y copies n floats from src to
+// dst (a batch's fields from the members' pinned staging, which the device
+// reads directly, and its results into one buffer for one copy to the host).
+struct CopySeg {
     const float *src;
-    long long off, n;
+    float *dst;
+    long long n;
 };
-static __global__ void k_pack(const PackSeg *segs, float *dst) {
-    const PackSeg s = segs[blockIdx.y];
+static __global__ void k_copy_segs(const CopySeg *segs) {
+    const CopySeg s = segs[blockIdx.y];
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < s.n; i += (long long)gridDim.x * blockDim.x)
-        dst[s.off + i] = s.src[i];
+        s.dst[i] = s.src[i];
 }
 
 struct SlotCommon {
@@ -989,25 +991,15 @@ struct Impl : ImplBase {
         return RC_OK;
     }
 
-    // Everything up to the march on stream st: field copy, set-up kernels
-    // and the descriptor (built into s.h_desc, copied to s.d_desc).
-    int prepare(Slot<R> &s, const float *T_dev, int zstart, int rpt, cudaStream_t st) {
+    // Host half of a solve's preparation: the descriptor (s.h_desc) and the
+    // tally outputs (s.h_out); no device work.
+    int prepare_host(Slot<R> &s, int zstart, int rpt) {
         std::string *err_ = &c->err;
-        const rc_params &p = c->p;
-        RC_FAILPOINT("field_copy");
         int rc = ensure_partial(s, rpt);
-        if (rc) return rc;
-        const size_t nfield = (size_t)(p.imax + 2) * (p.jmax + 2) * (p.kmax + 2);
-        if (T_dev) RC_CK(cudaMemcpyAsync(s.d_T, T_dev, nfield * sizeof(float), cudaMemcpyDeviceToDevice, st));
-        else RC_CK(cudaMemcpyAsync(s.d_T, s.h_T, nfield * sizeof(float), cudaMemcpyHostToDevice, st));
-        rc = enqueue_setup(s, st);
         if (rc) return rc;
         fill_desc(s, zstart, rpt, *s.h_desc);
         if (!decomposition_fits(*s.h_desc))
             return set_err(err_, RC_E_INVALID, "too many work items for one solve: raise rays_per_thread");
-        RC_CK(cudaMemcpyAsync(s.d_desc, s.h_desc, sizeof(DSolve<R>), cudaMemcpyHostToDevice, st));
-        k_patch_desc<R><<<1, 32, 0, st>>>(s.d_desc, s.d_sc);
-        RC_CK(cudaGetLastError());
         TallyOut *o = s.h_out;
         o->q64 = s.d_q64;
         o->var64 = s.d_var64;
@@ -1017,10 +1009,46 @@ struct Impl : ImplBase {
         o->Sc = s.d_Sc;
         o->Wq = s.d_Wq;
         o->Ws = s.d_Ws;
-        RC_CK(cudaMemcpyAsync(s.d_out, s.h_out, sizeof(TallyOut), cudaMemcpyHostToDevice, st));
         s.zstart = zstart;
         s.rpt = rpt;
         return RC_OK;
+    }
+
+    // Device half on stream st: the field copy (from T_dev, else from the
+    // slot's pinned staging; none when the caller has filled s.d_T), the
+    // set-up kernels, and the descriptor at desc_dev patched with the run-time
+    // scalars.  A batch passes its own descriptor array, already copied from
+    // the members' s.h_desc; a single solve the slot's (copied here, with the
+    // tally outputs).
+    int prepare_device(Slot<R> &s, const float *T_dev, bool field_ready, DSolve<R> *desc_dev, cudaStream_t st) {
+        std::string *err_ = &c->err;
+        const rc_params &p = c->p;
+        RC_FAILPOINT("field_copy");
+        const size_t nfield = (size_t)(p.imax + 2) * (p.jmax + 2) * (p.kmax + 2);
+        if (T_dev) RC_CK(cudaMemcpyAsync(s.d_T, T_dev, nfield * sizeof(float), cudaMemcpyDeviceToDevice, st));
+        else if (!field_ready) RC_CK(cudaMemcpyAsync(s.d_T, s.h_T, nfield * sizeof(float), cudaMemcpyHostToDevice, st));
+        int rc = enqueue_setup(s, st);
+        if (rc) return rc;
+        if (desc_dev == s.d_desc) {
+            RC_CK(cudaMemcpyAsync(s.d_desc, s.h_desc, sizeof(DSolve<R>), cudaMemcpyHostToDevice, st));
+            RC_CK(cudaMemcpyAsync(s.d_out, s.h_out, sizeof(TallyOut), cudaMemcpyHostToDevice, st));
+        }
+        k_patch_desc<R><<<1, 32, 0, st>>>(desc_dev, s.d_sc);
+        RC_CK(cudaGetLastError());
+        return RC_OK;
+    }
+
+    // Everything up to the march on stream st: field copy, set-up kernels
+    // and the descriptor (built into s.h_desc, copied to s.d_desc).
+    int prepare(Slot<R> &s, const float *T_dev, int zstart, int rpt, cudaStream_t st) {
+        int rc = prepare_host(s, zstart, rpt);
+        if (rc) return rc;
+        return prepare_device(s, T_dev, false, s.d_desc, st);
+    }
+
+    size_t field_floats() const {
+        const rc_params &p = c->p;
+        return (size_t)(p.imax + 2) * (p.jmax + 2) * (p.kmax + 2);
     }
 
     int launch_tally(const DSolve<R> *d_solves, const TallyOut *d_outs, int nsolves, long long max_cells,
@@ -1228,13 +1256,13 @@ struct Impl : ImplBase {
     size_t packed_floats() const {
         return (size_t)2 * c->p.imax * c->p.jmax * c->kloc + (size_t)4 * c->p.jmax * c->kloc;
     }
-    void pack_segments(Slot<R> &s, long long off, PackSeg *seg) const {
+    void pack_segments(Slot<R> &s, float *dst, CopySeg *seg) const {
         const long long ncf = (long long)c->p.imax * c->p.jmax * c->kloc;
         const long long nwc = 2LL * c->p.jmax * c->kloc;
-        seg[0] = PackSeg{s.d_Qc, off, ncf};
-        seg[1] = PackSeg{s.d_Sc, off + ncf, ncf};
-        seg[2] = PackSeg{s.d_Wq, off + 2 * ncf, nwc};
-        seg[3] = PackSeg{s.d_Ws, off + 2 * ncf + nwc, nwc};
+        seg[0] = CopySeg{s.d_Qc, dst, ncf};
+        seg[1] = CopySeg{s.d_Sc, dst + ncf, ncf};
+        seg[2] = CopySeg{s.d_Wq, dst + 2 * ncf, nwc};
+        seg[3] = CopySeg{s.d_Ws, dst + 2 * ncf + nwc, nwc};
     }
 
     void scatter_from(const float *Qc, const float *Sc, const float *Wq, const float *Ws, float *Q, float *sigma) {

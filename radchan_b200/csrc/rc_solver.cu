@@ -382,7 +382,7 @@ struct rc_batch {
     size_t cap = 0;
     // the members' float results gathered into one buffer and copied to
     // the host once per run (k_pack + one cudaMemcpyAsync)
-    PackSeg *d_segs = nullptr, *h_segs = nullptr;
+    CopySeg *d_segs = nullptr, *h_segs = nullptr;  // n field segments, then 4 n result segments
     float *d_pack = nullptr, *h_pack = nullptr;
     size_t pack_cap = 0;
     std::vector<size_t> pack_off;
@@ -399,7 +399,7 @@ namespace {
 template <typename R>
 int batch_reserve(rc_batch *b, size_t n) {
     std::string *err_ = &b->err;
-    if (4 * n > 65535) return set_err(err_, RC_E_INVALID, "more than 16383 solves in one batch");
+    if (5 * n > 65535) return set_err(err_, RC_E_INVALID, "more than 13107 solves in one batch");
     if (n <= b->cap) return RC_OK;
     if (b->d_solves) cudaFree(b->d_solves);
     if (b->h_solves) cudaFreeHost(b->h_solves);
@@ -416,8 +416,8 @@ int batch_reserve(rc_batch *b, size_t n) {
     if (b->d_segs) cudaFree(b->d_segs);
     if (b->h_segs) cudaFreeHost(b->h_segs);
     b->d_segs = b->h_segs = nullptr;
-    RC_CK(cudaMalloc((void **)&b->d_segs, 4 * n * sizeof(PackSeg)));
-    RC_CK(cudaHostAlloc((void **)&b->h_segs, 4 * n * sizeof(PackSeg), cudaHostAllocDefault));
+    RC_CK(cudaMalloc((void **)&b->d_segs, 5 * n * sizeof(CopySeg)));
+    RC_CK(cudaHostAlloc((void **)&b->h_segs, 5 * n * sizeof(CopySeg), cudaHostAllocDefault));
     b->cap = n;
     return RC_OK;
 }
@@ -462,9 +462,35 @@ int batch_enqueue(rc_batch *b, bool capturing) {
     int rpt_max = 1, block = 256, scat = 0;
     long long max_cells = 1;
     b->h_tiles[0] = 0;
-    // every member's field copy and set-up kernels, round-robin over the side
-    // streams: independent chains that run side by side (a member's chain is
-    // a dozen small launches; one after another they took ~110 us each)
+    // host halves: descriptors, tile prefix, tally outputs of every member
+    long long maxf = 1;
+    for (size_t i = 0; i < n; ++i) {
+        rc_ctx *c = b->m[i].ctx;
+        Impl<R> &im = *static_cast<Impl<R> *>(c->impl);
+        if (im.nA > 0) scat = 1;  // the scattering variant of the march serves every member
+        Slot<R> &s = *static_cast<Slot<R> *>(b->m[i].slot);
+        rc = im.prepare_host(s, b->m[i].zstart, c->rpt);
+        if (rc) return set_err(err_, rc, c->err);
+        hs[i] = *s.h_desc;
+        b->h_outs[i] = *s.h_out;
+        b->h_tiles[i + 1] = b->h_tiles[i] + s.h_desc->n_tiles;
+        rpt_max = std::max(rpt_max, c->rpt);
+        if (i == 0) block = c->block;
+        max_cells = std::max(max_cells, im.tally_cells());
+        b->h_segs[i] = CopySeg{s.h_T, s.d_T, (long long)im.field_floats()};
+        maxf = std::max(maxf, b->h_segs[i].n);
+    }
+    // one copy each of the descriptors, tile prefix and tally outputs; every
+    // member's field in one launch that reads the pinned staging directly
+    RC_CK(cudaMemcpyAsync(b->d_solves, hs, n * sizeof(DSolve<R>), cudaMemcpyHostToDevice, b->st));
+    RC_CK(cudaMemcpyAsync(b->d_tiles, b->h_tiles, (n + 1) * sizeof(long long), cudaMemcpyHostToDevice, b->st));
+    RC_CK(cudaMemcpyAsync(b->d_outs, b->h_outs, n * sizeof(TallyOut), cudaMemcpyHostToDevice, b->st));
+    RC_CK(cudaMemcpyAsync(b->d_segs, b->h_segs, n * sizeof(CopySeg), cudaMemcpyHostToDevice, b->st));
+    k_copy_segs<<<dim3((unsigned)std::min<long long>((maxf + 255) / 256, 64), (unsigned)n), 256, 0, b->st>>>(b->d_segs);
+    RC_CK(cudaGetLastError());
+    // every member's set-up kernels, round-robin over the side streams:
+    // independent chains that run side by side, patching the batch's
+    // descriptors in place
     const int ns = (int)std::min<size_t>(n, (size_t)rc_batch::kSideStreams);
     RC_CK(cudaEventRecord(b->fork, b->st));
     for (int k = 0; k < ns; ++k) RC_CK(cudaStreamWaitEvent(b->side[k], b->fork, 0));
@@ -472,33 +498,15 @@ int batch_enqueue(rc_batch *b, bool capturing) {
     for (size_t i = 0; i < n && !rc_members; ++i) {
         rc_ctx *c = b->m[i].ctx;
         Impl<R> &im = *static_cast<Impl<R> *>(c->impl);
-        if (im.nA > 0) scat = 1;  // the scattering variant of the march serves every member
         Slot<R> &s = *static_cast<Slot<R> *>(b->m[i].slot);
-        rc = im.prepare(s, nullptr, b->m[i].zstart, c->rpt, b->side[i % ns]);
-        if (rc) {
-            rc_members = set_err(err_, rc, c->err);
-            break;
-        }
-        hs[i] = *s.h_desc;
-        b->h_outs[i] = *s.h_out;
-        b->h_tiles[i + 1] = b->h_tiles[i] + s.h_desc->n_tiles;
-        rpt_max = std::max(rpt_max, c->rpt);
-        if (i == 0) block = c->block;
-        max_cells = std::max(max_cells, im.tally_cells());
+        rc = im.prepare_device(s, nullptr, true, static_cast<DSolve<R> *>(b->d_solves) + i, b->side[i % ns]);
+        if (rc) rc_members = set_err(err_, rc, c->err);
     }
     for (int k = 0; k < ns; ++k) {
         RC_CK(cudaEventRecord(b->join[k], b->side[k]));
         RC_CK(cudaStreamWaitEvent(b->st, b->join[k], 0));
     }
     if (rc_members) return rc_members;
-    // descriptors with their run-time fields already patched on the device
-    for (size_t i = 0; i < n; ++i) {
-        Slot<R> &s = *static_cast<Slot<R> *>(b->m[i].slot);
-        RC_CK(cudaMemcpyAsync(static_cast<DSolve<R> *>(b->d_solves) + i, s.d_desc, sizeof(DSolve<R>),
-                              cudaMemcpyDeviceToDevice, b->st));
-    }
-    RC_CK(cudaMemcpyAsync(b->d_tiles, b->h_tiles, (n + 1) * sizeof(long long), cudaMemcpyHostToDevice, b->st));
-    RC_CK(cudaMemcpyAsync(b->d_outs, b->h_outs, n * sizeof(TallyOut), cudaMemcpyHostToDevice, b->st));
     Impl<R> &im0 = *static_cast<Impl<R> *>(b->m[0].ctx->impl);
     RC_CK(mark(b->e_setup));
     rc = im0.launch_march(static_cast<const DSolve<R> *>(b->d_solves), b->d_tiles, (int)n, b->h_tiles[n],
@@ -509,18 +517,19 @@ int batch_enqueue(rc_batch *b, bool capturing) {
     if (rc) return set_err(err_, rc, b->m[0].ctx->err);
     // float results of every member into one buffer, one copy to the host
     long long maxn = 1;
+    CopySeg *rs = b->h_segs + n;
     for (size_t i = 0; i < n; ++i) {
         Impl<R> &im = *static_cast<Impl<R> *>(b->m[i].ctx->impl);
-        im.pack_segments(*static_cast<Slot<R> *>(b->m[i].slot), (long long)b->pack_off[i], b->h_segs + 4 * i);
-        for (int q = 0; q < 4; ++q) maxn = std::max(maxn, b->h_segs[4 * i + q].n);
+        im.pack_segments(*static_cast<Slot<R> *>(b->m[i].slot), b->d_pack + b->pack_off[i], rs + 4 * i);
+        for (int q = 0; q < 4; ++q) maxn = std::max(maxn, rs[4 * i + q].n);
     }
     size_t floats = 0;
     for (size_t i = 0; i < n; ++i)
         floats += static_cast<Impl<R> *>(b->m[i].ctx->impl)->packed_floats();
-    RC_CK(cudaMemcpyAsync(b->d_segs, b->h_segs, 4 * n * sizeof(PackSeg), cudaMemcpyHostToDevice, b->st));
+    RC_CK(cudaMemcpyAsync(b->d_segs + n, rs, 4 * n * sizeof(CopySeg), cudaMemcpyHostToDevice, b->st));
     {
         const int gx = (int)std::min<long long>((maxn + 255) / 256, 64);
-        k_pack<<<dim3(gx, (unsigned)(4 * n)), 256, 0, b->st>>>(b->d_segs, b->d_pack);
+        k_copy_segs<<<dim3(gx, (unsigned)(4 * n)), 256, 0, b->st>>>(b->d_segs + n);
         RC_CK(cudaGetLastError());
     }
     RC_CK(cudaMemcpyAsync(b->h_pack, b->d_pack, floats * sizeof(float), cudaMemcpyDeviceToHost, b->st));
