@@ -297,10 +297,8 @@ int rc_get_launch(rc_ctx *ctx, int *rays_per_thread, int *block_threads, int *so
  * never a result.  Each solve slot builds the list on its first solve and
  * reuses it while the draws and the work decomposition stay the same (seed,
  * photmax, rays_per_thread, replicates, grid, walls, threshold): a later
- * field can only make the order less apt.  It is used only when no other
- * solve of the context is still running on the device (that solve fills
- * the tail anyway), and solves of more than 2^22 tiles skip it (there,
- * reordering cost more than the tail it removed). */
+ * field can only make the order less apt.  Solves of more than 2^22 tiles
+ * skip it (there, reordering cost more than the tail it removed). */
 #define RC_PRIORITY_DEFAULT 12.0f
 int rc_set_priority(rc_ctx *ctx, float threshold);
 /* Try launch configurations on T (host) with a reduced bundle count

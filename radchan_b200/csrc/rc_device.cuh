@@ -674,24 +674,26 @@ __device__ __forceinline__ int march_step(Ray<R> &r, ScatState<R> &qs, const DSo
     R ds = dsx;
     if (ds > dsy) ds = dsy;
     if (ds > dsz) ds = dsz;
+    // with SCAT, ev: the next scattering event lies inside this cell; the
+    // bundle stops there (one absorption path shared with the plain step,
+    // so the step loop's code does not grow)
+    R dstep = ds;
+    bool ev = false;
     if constexpr (SCAT) {
-        if (ds > qs.dist) {
-            // the next scattering event lies inside this cell
-            const R dsc = qs.dist;
-            r.xp = RT<R>::fma_(dsc, r.sx, r.xp);
-            r.yp = RT<R>::fma_(dsc, r.sy, r.yp);
-            r.zp = RT<R>::fma_(dsc, r.sz, r.zp);
-            absorb(r, dsc, absco, blackpow);
-            qs.dist = (R)-1;
+        ev = ds > qs.dist;
+        dstep = ev ? qs.dist : ds;
+        qs.dist = ev ? (R)-1 : qs.dist - ds;
+    }
+    r.xp = (!ev && ds == dsx) ? fxu : RT<R>::fma_(dstep, r.sx, r.xp);
+    r.yp = (!ev && ds == dsy) ? fyu : RT<R>::fma_(dstep, r.sy, r.yp);
+    r.zp = (!ev && ds == dsz) ? fzu : RT<R>::fma_(dstep, r.sz, r.zp);
+    absorb(r, dstep, absco, blackpow);
+    if constexpr (SCAT) {
+        if (ev) {
             r.counter += 1;
             return B.w;
         }
-        qs.dist = qs.dist - ds;
     }
-    r.xp = (ds == dsx) ? fxu : RT<R>::fma_(ds, r.sx, r.xp);
-    r.yp = (ds == dsy) ? fyu : RT<R>::fma_(ds, r.sy, r.yp);
-    r.zp = (ds == dsz) ? fzu : RT<R>::fma_(ds, r.sz, r.zp);
-    absorb(r, ds, absco, blackpow);
     // crossed axis (ties: x only if strictly smallest, :375-377, 524)
     const int axis = (dsx < dsy) ? ((dsx < dsz) ? 0 : 2) : ((dsy < dsz) ? 1 : 2);
     const bool ax0 = axis == 0, ax1 = axis == 1;

@@ -1085,17 +1085,13 @@ struct Impl : ImplBase {
         s.h_tiles[0] = 0;
         s.h_tiles[1] = s.h_desc->n_tiles;
         RC_CK(cudaMemcpyAsync(s.d_tiles, s.h_tiles, 2 * sizeof(long long), cudaMemcpyHostToDevice, s.st));
-        // the long-ray priority pays only when this solve is alone on the
-        // device: a solve still running in the other slot overlaps its tail
-        bool alone = true;
-        for (auto &o : slots)
-            if (&o != &s && o.state == 1 && cudaEventQuery(o.e1) == cudaErrorNotReady) alone = false;
+        // the long-ray priority list (built once per slot, then reused):
+        // also while the other slot's solve runs, where it measured 28.1 ms
+        // per solve end to end against 28.8-29.1 ms without it
         RC_CK(cudaEventRecord(s.e_march0, s.st));
         bool prio = false;
-        if (alone) {
-            rc = enqueue_prio(s, s.st, prio);
-            if (rc) return rc;
-        }
+        rc = enqueue_prio(s, s.st, prio);
+        if (rc) return rc;
         rc = launch_march(s.d_desc, s.d_tiles, 1, s.h_desc->n_tiles, s.d_counter, c->block, rpt, s.st, 0,
                           prio ? &s : nullptr);
         if (rc) return rc;
