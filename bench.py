@@ -599,6 +599,8 @@ def leg_batched(dev, passes=2, tol=None, max_bundles=2.5e11, served=True, warm=T
         n = len(items)
         return {"problems": n, "bundles_per_pass": bundles, "tolerance": tol,
                 "photmax_range": [min(it["p"].photmax for it in items), max(it["p"].photmax for it in items)],
+                "autotuned": {"rays_per_thread": knobs[0], "block_threads": knobs[1], "sort_bands": knobs[2],
+                              "occupancy": knobs[3]},
                 "plain_solves_per_s": n / t_plain, "batched_solves_per_s": n / t_batch,
                 "batched_vs_plain": t_plain / t_batch, "plain_bundles_per_s": bundles / t_plain,
                 "batched_bundles_per_s": bundles / t_batch, "steps_per_pass": steps,

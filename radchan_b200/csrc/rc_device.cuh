@@ -580,17 +580,20 @@ __device__ __forceinline__ R scatter_first_dist(const DSolve<R> &S, uint4 ctr, R
     return dist;
 }
 
-// New direction at the next scattering event of a bundle in band r.nb (ctr:
-// its counter words x, y, z and the number of events so far in w; ks > 0 its
-// scattering coefficient), and the free path to the event after it.  The direction is turned by the
-// sampled polar angle theta about the old one, with azimuth phi measured
-// from the plane of the old direction and the z axis (the standard rotation
-// of Monte Carlo transport codes; near |s_z| = 1 the new direction is taken
-// about the z axis itself).  Zero components are floored to 1e-10 as at
-// emission (:132-137).
+// New direction of a bundle travelling along (sx, sy, sz) in band nb at a
+// scattering event (ctr: its counter words x, y, z and the number of the
+// event in w; ks > 0 its scattering coefficient), with the reciprocals of
+// the new direction and the free path to the event after it.  Everything is
+// passed and returned by value: the function is not inlined (it is rare and
+// long), and a reference would oblige the caller to keep the ray in local
+// memory.
 template <typename R>
-__device__ __noinline__ void scatter_turn(Ray<R> &r, uint4 &ctr, R ks, ScatState<R> &q, const DSolve<R> &S) {
-    ctr.w += 1u;
+struct TurnOut {
+    R sx, sy, sz, isx, isy, isz, dist;
+};
+template <typename R>
+__device__ __noinline__ TurnOut<R> scatter_turn_v(R sx, R sy, R sz, int nb, uint4 ctr, R ks, const DSolve<R> *Sp) {
+    const DSolve<R> &S = *Sp;
     rc_u32x4 c;
     c.x = ctr.x;
     c.y = ctr.y;
@@ -599,7 +602,7 @@ __device__ __noinline__ void scatter_turn(Ray<R> &r, uint4 &ctr, R ks, ScatState
     const rc_u32x4 d = rc_philox4x32_10(c, S.key0, S.key1);
     const R u_t = (R)rc_u01(d.x), u_p = (R)rc_u01(d.y), u_s = (R)rc_u01(d.z);
     const int nA = S.nA;
-    const R *cdf = S.pcdf + RC_IX((size_t)r.nb * nA, (long long)S.nB * nA, SITE_PHASE, S);
+    const R *cdf = S.pcdf + RC_IX((size_t)nb * nA, (long long)S.nB * nA, SITE_PHASE, S);
     int lo = 0, hi = nA - 1;
     while (hi - lo > 1) {
         const int mid = (lo + hi) >> 1;
@@ -615,27 +618,44 @@ __device__ __noinline__ void scatter_turn(Ray<R> &r, uint4 &ctr, R ks, ScatState
     RT<R>::sincos2pi_(th, &st, &ct);
     RT<R>::sincos2pi_(u_p, &sp, &cp);
     R nx, ny, nz;
-    if (RT<R>::fabs_(r.sz) > (R)0.99999) {
+    if (RT<R>::fabs_(sz) > (R)0.99999) {
         nx = st * cp;
         ny = st * sp;
-        nz = (r.sz > (R)0) ? ct : -ct;
+        nz = (sz > (R)0) ? ct : -ct;
     } else {
-        const R w = RT<R>::sqrt_((R)1 - r.sz * r.sz);
+        const R w = RT<R>::sqrt_((R)1 - sz * sz);
         const R a = st / w;
-        nx = a * (r.sx * r.sz * cp - r.sy * sp) + r.sx * ct;
-        ny = a * (r.sy * r.sz * cp + r.sx * sp) + r.sy * ct;
-        nz = r.sz * ct - st * cp * w;
+        nx = a * (sx * sz * cp - sy * sp) + sx * ct;
+        ny = a * (sy * sz * cp + sx * sp) + sy * ct;
+        nz = sz * ct - st * cp * w;
     }
     if (nx == (R)0) nx = (R)1e-10;
     if (ny == (R)0) ny = (R)1e-10;
     if (nz == (R)0) nz = (R)1e-10;
-    r.sx = nx;
-    r.sy = ny;
-    r.sz = nz;
-    r.isx = (R)1 / nx;
-    r.isy = (R)1 / ny;
-    r.isz = (R)1 / nz;
-    q.dist = -RT<R>::log_(u_s) / ks;
+    TurnOut<R> o;
+    o.sx = nx;
+    o.sy = ny;
+    o.sz = nz;
+    o.isx = (R)1 / nx;
+    o.isy = (R)1 / ny;
+    o.isz = (R)1 / nz;
+    o.dist = -RT<R>::log_(u_s) / ks;
+    return o;
+}
+
+// The next scattering event of ray r: the event count in ctr.w advances,
+// the direction turns, and q receives the free path to the event after it.
+template <typename R>
+__device__ __forceinline__ void scatter_turn(Ray<R> &r, uint4 &ctr, R ks, ScatState<R> &q, const DSolve<R> &S) {
+    ctr.w += 1u;
+    const TurnOut<R> o = scatter_turn_v(r.sx, r.sy, r.sz, r.nb, ctr, ks, &S);
+    r.sx = o.sx;
+    r.sy = o.sy;
+    r.sz = o.sz;
+    r.isx = o.isx;
+    r.isy = o.isy;
+    r.isz = o.isz;
+    q.dist = o.dist;
 }
 
 // One ray-cell crossing (one iteration of the while loop of march_ray,

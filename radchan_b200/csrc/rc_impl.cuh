@@ -669,8 +669,8 @@ struct Impl : ImplBase {
 
     // Work decomposition: items of rpt bundles, chunk count padded so that
     // the chunks of one (cell, replicate) never straddle a 32-item tile.
-    void decompose(int rpt, int &nchunk, int &gsize, int &nparts) const {
-        const int photmax = c->p.photmax;
+    void decompose(int rpt, int &nchunk, int &gsize, int &nparts, int photmax = 0) const {
+        if (photmax <= 0) photmax = c->p.photmax;
         int nc = (photmax + rpt - 1) / rpt;
         if (nc <= kWarp) {
             int p2 = 1;
@@ -804,9 +804,9 @@ struct Impl : ImplBase {
         return ok;
     }
 
-    size_t partial_count(int rpt) const {
+    size_t partial_count(int rpt, int photmax = 0) const {
         int nchunk, gsize, nparts;
-        decompose(rpt, nchunk, gsize, nparts);
+        decompose(rpt, nchunk, gsize, nparts, photmax);
         const rc_params &p = c->p;
         const long long ncells = (long long)p.imax * p.jmax * c->kloc + 2LL * p.jmax * c->kloc;
         return (size_t)ncells * p.nVar * nparts;
@@ -1112,10 +1112,12 @@ struct Impl : ImplBase {
     // not change the sampled bundles (counter-based draws), only the work
     // decomposition, the FP64 summation grouping and the order in which a
     // warp's lanes take bundles.
+    // March time of one launch configuration on the pilot: the best of two
+    // timed launches after a warm-up launch.
     int time_config(Slot<R> &s, int zstart, int rpt, int block, int minb, float *ms_out) {
         std::string *err_ = &c->err;
-        float tot = 0.f;
-        for (int rep = 0; rep < 2; ++rep) {
+        float tot = 3.4e38f;
+        for (int rep = 0; rep < 3; ++rep) {
             int rc = prepare(s, nullptr, zstart, rpt, s.st);
             if (rc) return rc;
             s.h_tiles[0] = 0;
@@ -1132,7 +1134,7 @@ struct Impl : ImplBase {
             RC_CK(cudaEventSynchronize(s.e_march1));
             float ms = 0.f;
             RC_CK(cudaEventElapsedTime(&ms, s.e_march0, s.e_march1));
-            if (rep > 0) tot += ms;  // the first run warms up
+            if (rep > 0) tot = std::min(tot, ms);  // the first run warms up
         }
         *ms_out = tot;
         return RC_OK;
@@ -1148,22 +1150,43 @@ struct Impl : ImplBase {
         Slot<R> &s = *sp;
         const int saved_photmax = c->p.photmax, saved_sort = c->sort;
         if (pilot > 0) c->p.photmax = pilot;
+        const double scale = (double)saved_photmax / (double)c->p.photmax;
         rc = stage_host_field(s, T);
-        float best = 3.4e38f;
+        // Estimated time of the real solve: the pilot's march scaled by the
+        // bundle count, plus writing and reading the FP64 partial sums at the
+        // real photmax (a pilot has few; at a large photmax a small
+        // rays_per_thread makes them gigabytes).
+        int mem_khz = 0, bus_bits = 0;
+        cudaDeviceGetAttribute(&mem_khz, cudaDevAttrMemoryClockRate, c->device);
+        cudaDeviceGetAttribute(&bus_bits, cudaDevAttrGlobalMemoryBusWidth, c->device);
+        const double hbm = (mem_khz > 0 && bus_bits > 0) ? 2.0 * mem_khz * 1e3 * bus_bits / 8.0 : 6.5e12;
+        auto estimate = [&](float ms_pilot, int rpt) {
+            return ms_pilot * scale + 2.0 * 8.0 * (double)partial_count(rpt, saved_photmax) / hbm * 1e3;
+        };
+        // the current knobs are the incumbent; another configuration must
+        // beat it by 3 % to replace it (pilot timings vary by about that)
+        c->sort = 0;
         int brpt = c->rpt, bblock = c->block, bminb = c->minb, bsort = 0;
+        double best = 1e300;
+        if (!rc && march_smem(bblock, brpt, nA > 0) <= (size_t)smem_opt_in) {
+            float ms = 0.f;
+            rc = time_config(s, zstart, brpt, bblock, bminb, &ms);
+            if (!rc) best = estimate(ms, brpt);
+        }
         const int rpts[] = {2, 4, 8, 16, 32};
         const int blocks[] = {128, 256};
         const int minbs[] = {2, 3, 4};
-        c->sort = 0;
         for (int oi = 0; oi < 3 && !rc; ++oi)
             for (int bi = 0; bi < 2 && !rc; ++bi)
                 for (int ri = 0; ri < 5 && !rc; ++ri) {
                     const int rpt = rpts[ri], block = blocks[bi], minb = minbs[oi];
+                    if (rpt == brpt && block == bblock && minb == bminb) continue;
                     if (march_smem(block, rpt, nA > 0) > (size_t)smem_opt_in) continue;
                     float ms = 0.f;
                     rc = time_config(s, zstart, rpt, block, minb, &ms);
-                    if (!rc && ms < best) {
-                        best = ms;
+                    const double e = estimate(ms, rpt);
+                    if (!rc && e < 0.97 * best) {
+                        best = e;
                         brpt = rpt;
                         bblock = block;
                         bminb = minb;
@@ -1173,7 +1196,7 @@ struct Impl : ImplBase {
             c->sort = 1;
             float ms = 0.f;
             rc = time_config(s, zstart, brpt, bblock, bminb, &ms);
-            if (!rc && ms < best) bsort = 1;
+            if (!rc && estimate(ms, brpt) < 0.97 * best) bsort = 1;
         }
         c->p.photmax = saved_photmax;
         if (rc) {
