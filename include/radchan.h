@@ -306,10 +306,13 @@ int rc_set_priority(rc_ctx *ctx, float threshold);
  * rays_per_thread x block_threads x occupancy with sorting off, then
  * sort_bands on at the best of those.  Each configuration is scored by the
  * estimated time of the real solve: its pilot march time (best of two
- * launches after a warm-up) scaled to the context's photmax, plus writing
- * and reading the FP64 partial sums that rays_per_thread implies at that
- * photmax.  The current knobs are the incumbent, and another configuration
- * must beat them by 3 %.  Writes the chosen knobs. */
+ * launches after a warm-up) scaled to the context's photmax -- when that is
+ * more than 4x the pilot, from the pilot timed at one and at two times its
+ * photmax, so the marginal cost per bundle carries the estimate and not the
+ * pilot's tail -- plus writing and reading the FP64 partial sums that
+ * rays_per_thread implies at that photmax.  The current knobs are the
+ * incumbent, and another configuration must beat them by 3 %.  Writes the
+ * chosen knobs. */
 int rc_autotune(rc_ctx *ctx, const float *T, int zstart, int pilot_photmax,
                 int *rays_per_thread, int *block_threads, int *sort_bands, int *occupancy);
 /* Solve without allocating device memory (this entry point has no

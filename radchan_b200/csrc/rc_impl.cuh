@@ -1150,29 +1150,42 @@ struct Impl : ImplBase {
         Slot<R> &s = *sp;
         const int saved_photmax = c->p.photmax, saved_sort = c->sort;
         if (pilot > 0) c->p.photmax = pilot;
-        const double scale = (double)saved_photmax / (double)c->p.photmax;
+        const int p1 = c->p.photmax;
         rc = stage_host_field(s, T);
-        // Estimated time of the real solve: the pilot's march scaled by the
-        // bundle count, plus writing and reading the FP64 partial sums at the
-        // real photmax (a pilot has few; at a large photmax a small
-        // rays_per_thread makes them gigabytes).
+        // Estimated time of the real solve.  A pilot's launch carries a tail
+        // (its last, longest rays) that a long solve hides, so a pilot much
+        // smaller than the real photmax is timed at p1 and 2 p1 bundles per
+        // cell: t(P) = t(p1) + (t(2 p1) - t(p1)) (P - p1) / p1, the marginal
+        // cost per bundle carrying the estimate.  Writing and reading the FP64
+        // partial sums that rays_per_thread implies at the real photmax is
+        // added.
+        const bool two_point = saved_photmax > 4 * p1;
         int mem_khz = 0, bus_bits = 0;
         cudaDeviceGetAttribute(&mem_khz, cudaDevAttrMemoryClockRate, c->device);
         cudaDeviceGetAttribute(&bus_bits, cudaDevAttrGlobalMemoryBusWidth, c->device);
         const double hbm = (mem_khz > 0 && bus_bits > 0) ? 2.0 * mem_khz * 1e3 * bus_bits / 8.0 : 6.5e12;
-        auto estimate = [&](float ms_pilot, int rpt) {
-            return ms_pilot * scale + 2.0 * 8.0 * (double)partial_count(rpt, saved_photmax) / hbm * 1e3;
+        auto score = [&](int rpt, int block, int minb, double *est) {
+            float t1 = 0.f;
+            int r = time_config(s, zstart, rpt, block, minb, &t1);
+            if (r) return r;
+            double e = (double)t1 * saved_photmax / p1;
+            if (two_point) {
+                float t2 = 0.f;
+                c->p.photmax = 2 * p1;
+                r = time_config(s, zstart, rpt, block, minb, &t2);
+                c->p.photmax = p1;
+                if (r) return r;
+                e = (double)t1 + std::max(0.0, (double)t2 - (double)t1) * (double)(saved_photmax - p1) / p1;
+            }
+            *est = e + 2.0 * 8.0 * (double)partial_count(rpt, saved_photmax) / hbm * 1e3;
+            return RC_OK;
         };
         // the current knobs are the incumbent; another configuration must
         // beat it by 3 % to replace it (pilot timings vary by about that)
         c->sort = 0;
         int brpt = c->rpt, bblock = c->block, bminb = c->minb, bsort = 0;
         double best = 1e300;
-        if (!rc && march_smem(bblock, brpt, nA > 0) <= (size_t)smem_opt_in) {
-            float ms = 0.f;
-            rc = time_config(s, zstart, brpt, bblock, bminb, &ms);
-            if (!rc) best = estimate(ms, brpt);
-        }
+        if (!rc && march_smem(bblock, brpt, nA > 0) <= (size_t)smem_opt_in) rc = score(brpt, bblock, bminb, &best);
         const int rpts[] = {2, 4, 8, 16, 32};
         const int blocks[] = {128, 256};
         const int minbs[] = {2, 3, 4};
@@ -1182,9 +1195,8 @@ struct Impl : ImplBase {
                     const int rpt = rpts[ri], block = blocks[bi], minb = minbs[oi];
                     if (rpt == brpt && block == bblock && minb == bminb) continue;
                     if (march_smem(block, rpt, nA > 0) > (size_t)smem_opt_in) continue;
-                    float ms = 0.f;
-                    rc = time_config(s, zstart, rpt, block, minb, &ms);
-                    const double e = estimate(ms, rpt);
+                    double e = 0.0;
+                    rc = score(rpt, block, minb, &e);
                     if (!rc && e < 0.97 * best) {
                         best = e;
                         brpt = rpt;
@@ -1194,9 +1206,9 @@ struct Impl : ImplBase {
                 }
         if (!rc) {
             c->sort = 1;
-            float ms = 0.f;
-            rc = time_config(s, zstart, brpt, bblock, bminb, &ms);
-            if (!rc && estimate(ms, brpt) < 0.97 * best) bsort = 1;
+            double e = 0.0;
+            rc = score(brpt, bblock, bminb, &e);
+            if (!rc && e < 0.97 * best) bsort = 1;
         }
         c->p.photmax = saved_photmax;
         if (rc) {
