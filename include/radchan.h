@@ -302,7 +302,8 @@ int rc_get_launch(rc_ctx *ctx, int *rays_per_thread, int *block_threads, int *so
 #define RC_PRIORITY_DEFAULT 12.0f
 int rc_set_priority(rc_ctx *ctx, float threshold);
 /* Try launch configurations on T (host) with a reduced bundle count
- * (pilot_photmax; <= 0: the context's photmax) and keep the fastest:
+ * (pilot_photmax, raised until a pilot launch has 10^8 bundles, at most the
+ * context's photmax; <= 0: the context's photmax) and keep the fastest:
  * rays_per_thread x block_threads x occupancy with sorting off, then
  * sort_bands on at the best of those.  Each configuration is scored by the
  * estimated time of the real solve: its pilot march time (best of two

@@ -1149,7 +1149,17 @@ struct Impl : ImplBase {
         if (!sp) return set_err(err_, RC_E_BUSY, "all solve slots in use");
         Slot<R> &s = *sp;
         const int saved_photmax = c->p.photmax, saved_sort = c->sort;
-        if (pilot > 0) c->p.photmax = pilot;
+        // the pilot is raised until its launch has 10^8 bundles or more
+        // (at most the real photmax): a shorter launch is dominated by its
+        // tail and launch latency, and ranks configurations by those
+        {
+            const rc_params &p = c->p;
+            const long long cellsv =
+                ((long long)p.imax * p.jmax * c->kloc + 2LL * p.jmax * c->kloc) * std::max(p.nVar, 1);
+            int pp = pilot > 0 ? std::min(pilot, saved_photmax) : saved_photmax;
+            while ((long long)pp * cellsv < 100000000LL && pp < saved_photmax) pp = std::min(2 * pp, saved_photmax);
+            c->p.photmax = pp;
+        }
         const int p1 = c->p.photmax;
         rc = stage_host_field(s, T);
         // Estimated time of the real solve.  A pilot's launch carries a tail

@@ -381,7 +381,7 @@ struct rc_batch {
     unsigned long long *d_counter = nullptr;
     size_t cap = 0;
     // the members' float results gathered into one buffer and copied to
-    // the host once per run (k_pack + one cudaMemcpyAsync)
+    // the host once per run (k_copy_segs + one cudaMemcpyAsync)
     CopySeg *d_segs = nullptr, *h_segs = nullptr;  // n field segments, then 4 n result segments
     float *d_pack = nullptr, *h_pack = nullptr;
     size_t pack_cap = 0;
