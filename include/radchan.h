@@ -234,8 +234,9 @@ int rc_set_tables(rc_ctx *ctx, const rc_tables *t);
  * the way as before; every draw comes from the bundle's own Philox counter
  * (emission's, with an event number), so results stay independent of the
  * launch shape.  Batches run such contexts in the scattering variant of the
- * march; the server serves media without scattering only.  Set it between
- * solves (no solve of the context in flight). */
+ * march; the server takes particles per table set
+ * (rc_server_set_scattering).  Set it between solves (no solve of the
+ * context in flight). */
 int rc_set_scattering(rc_ctx *ctx, const rc_scattering *s);
 /* Copy T (host, whole field incl. ghosts) and launch; returns at once. */
 int rc_solve_async(rc_ctx *ctx, const float *T, int zstart, rc_ticket *ticket);
@@ -401,19 +402,19 @@ int rc_probe_gather(int device, size_t bytes, int mode, int iters, double *secto
 typedef struct rc_batch rc_batch;
 /* A batch runs many contexts' solves (uneven grids, tables, photmax) in
  * one persistent work-queue launch; with use_graph the whole sequence
- * (copies + kernels) is captured once and replayed.  The long-ray priority
- * list (rc_set_priority) spans the whole batch when any member has it on
- * and the batch has at most 2^22 tiles: the march claims the tiles of every
- * member that hold a long ray first.  Every run also gathers the members'
- * float results (Q, sigma, wall fluxes) into one buffer copied to the host
- * once, so rc_batch_collect with only Q / sigma copies nothing more. */
+ * (copies + kernels) is captured once and replayed.  The members' fields
+ * are copied by one kernel, their set-up kernels run as parallel chains,
+ * and the march takes the tiles in natural order.  Every run also gathers
+ * the members' float results (Q, sigma, wall fluxes) into one buffer
+ * copied to the host once, so rc_batch_collect with only Q / sigma copies
+ * nothing more. */
 int rc_batch_create(int device, int use_graph, rc_batch **out);
 int rc_batch_add(rc_batch *b, rc_ctx *ctx, const float *T_host, int zstart);
 int rc_batch_run(rc_batch *b);          /* enqueue; returns at once */
 int rc_batch_wait(rc_batch *b, float *ms_device);
 /* Device time of the last run by phase: set-up of every member (field
- * copies, set-up kernels, priority list), the march, and tally plus result
- * copies.  Waits for the run. */
+ * copies, set-up kernels), the march, and tally plus result copies.  Waits
+ * for the run. */
 int rc_batch_phases(rc_batch *b, float *ms_setup, float *ms_march, float *ms_tally);
 int rc_batch_collect(rc_batch *b, int index, float *Q, float *sigma,
                      double *q64, double *var64, double *qw64, double *vw64);
@@ -437,6 +438,11 @@ typedef struct rc_result_info {
 } rc_result_info;
 int rc_server_create(int device, double hbm_budget_bytes, int max_inflight, rc_server **out);
 int rc_server_add_tables(rc_server *s, const rc_tables *t, int *table_set);
+/* Particle scattering for the requests of a table set (table_set -1: grey
+ * requests; NULL removes it), copied.  Requests submitted afterwards solve
+ * in that medium; a request keeps the particles current when it was
+ * submitted, and contexts are pooled per table set and particle set. */
+int rc_server_set_scattering(rc_server *s, int table_set, const rc_scattering *sc);
 int rc_server_submit(rc_server *s, const rc_request *req, int64_t *id);
 /* Wait for a request; Q/sigma in the Fortran result layout (may be NULL). */
 int rc_server_wait(rc_server *s, int64_t id, float *Q, float *sigma, rc_result_info *info);

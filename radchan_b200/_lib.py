@@ -163,6 +163,7 @@ _SIGS = [
     ("rc_batch_destroy", _I, [_VP]),
     ("rc_server_create", _I, [_I, C.c_double, _I, C.POINTER(_VP)]),
     ("rc_server_add_tables", _I, [_VP, C.POINTER(RcTables), C.POINTER(C.c_int)]),
+    ("rc_server_set_scattering", _I, [_VP, _I, C.POINTER(RcScattering)]),
     ("rc_server_submit", _I, [_VP, C.POINTER(RcRequest), C.POINTER(C.c_int64)]),
     ("rc_server_wait", _I, [_VP, C.c_int64, _FP, _FP, C.POINTER(RcResultInfo)]),
     ("rc_server_stats", _I, [_VP, _DP, _DP, _DP]),

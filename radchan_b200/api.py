@@ -540,6 +540,13 @@ class Server:
         self._tables.append(tables)
         return ts.value
 
+    def set_scattering(self, table_set: int, sc: "Scattering | None"):
+        """rc_server_set_scattering: particles for the later requests of a
+        table set (-1: grey requests); None removes them."""
+        self._scatter = getattr(self, "_scatter", {})
+        self._scatter[table_set] = sc
+        L.check(L.lib().rc_server_set_scattering(self.h, table_set, C.byref(sc.view) if sc is not None else None))
+
     def submit(self, params: L.RcParams, T: np.ndarray, table_set: int = -1, zstart: int = 1,
                tolerance: float = 0.0) -> int:
         p = copy_params(params)

@@ -67,6 +67,8 @@ struct SrvReq {
     rc_ctx *ctx = nullptr;
     Slot<float> *slot = nullptr;
     std::string key;
+    // particle scattering of the request's table set at submit time (null: none)
+    std::shared_ptr<const ScatterSet> scatter;
     long long tiles = 0, next_tile = 0;
     int photmax = 0;
     float rel_std = 0.f;
@@ -104,6 +106,10 @@ struct rc_server {
     int policy = RC_SCHED_SRPT;
     long long quanta = 0;
     std::vector<std::unique_ptr<TableSet>> tables;  // stable addresses: appended while the worker reads
+    // particle scattering per table set (-1: grey requests), replaced whole
+    // by rc_server_set_scattering; a request keeps the one current at submit
+    std::map<int, std::shared_ptr<const ScatterSet>> scatter;
+    std::map<int, int> scatter_gen;
     std::mutex mu;
     std::condition_variable cv_work, cv_done;
     std::deque<SrvReq *> queue;
@@ -281,6 +287,16 @@ int acquire_context(rc_server *sv, SrvReq *r) {
             return set_err(nullptr, rc, m);
         }
     }
+    if (r->scatter) {
+        rc_scattering sv_view;
+        r->scatter->view(&sv_view);
+        rc = rc_set_scattering(c, &sv_view);
+        if (rc) {
+            const std::string m = c->err;
+            rc_destroy(c);
+            return set_err(nullptr, rc, m);
+        }
+    }
     sv->pool.push_back(PoolCtx{c, need, r->key, true});
     std::lock_guard<std::mutex> lk(sv->mu);
     sv->hbm_in_use += need;
@@ -417,8 +433,11 @@ int run_quantum(rc_server *sv, const std::vector<SrvReq *> &marching, int par) {
     RC_CK(cudaEventRecord(sv->pre_done[par], st));
     if (ht[n] > 0) {
         Impl<float> &im0 = *static_cast<Impl<float> *>(marching[0]->ctx->impl);
+        int scat = 0;  // the scattering variant of the march when any request's medium scatters
+        for (int i = 0; i < n; ++i)
+            if (static_cast<Impl<float> *>(marching[i]->ctx->impl)->nA > 0) scat = 1;
         const int rc = im0.launch_march(sv->d_solves[par], sv->d_tiles[par], n, ht[n], sv->d_counter[par],
-                                        marching[0]->ctx->block, rpt_max, st);
+                                        marching[0]->ctx->block, rpt_max, st, 0, nullptr, scat);
         if (rc) return set_err(err_, rc, marching[0]->ctx->err);
     }
     RC_CK(cudaEventRecord(sv->mend[par], st));
@@ -696,6 +715,30 @@ int rc_server_create(int device, double hbm_budget_bytes, int max_inflight, rc_s
     return RC_OK;
 }
 
+int rc_server_set_scattering(rc_server *sv, int table_set, const rc_scattering *s) {
+    if (!sv) return set_err(nullptr, RC_E_INVALID, "NULL server");
+    std::shared_ptr<ScatterSet> ss;
+    if (s) {
+        std::string err;
+        if (scattering_check(*s, err)) return set_err(nullptr, RC_E_INVALID, err);
+        ss = std::make_shared<ScatterSet>();
+        ss->nB = s->nB;
+        ss->nQ = s->nQ;
+        ss->nA = s->nA;
+        ss->ksca.assign(s->ksca, s->ksca + (size_t)s->nB * s->nQ);
+        if (s->kabs) ss->kabs.assign(s->kabs, s->kabs + (size_t)s->nB * s->nQ);
+        ss->theta.assign(s->theta, s->theta + s->nA);
+        ss->cdf.assign(s->phase_cdf, s->phase_cdf + (size_t)s->nB * s->nA);
+    }
+    std::lock_guard<std::mutex> lk(sv->mu);
+    if (table_set < -1 || table_set >= (int)sv->tables.size())
+        return set_err(nullptr, RC_E_INVALID, "unknown table set");
+    if (ss) sv->scatter[table_set] = ss;
+    else sv->scatter.erase(table_set);
+    sv->scatter_gen[table_set] += 1;
+    return RC_OK;
+}
+
 int rc_server_add_tables(rc_server *sv, const rc_tables *t, int *table_set) {
     if (!sv || !t || !table_set) return set_err(nullptr, RC_E_INVALID, "NULL argument");
     auto ts = std::make_unique<TableSet>();
@@ -730,6 +773,13 @@ int rc_server_submit(rc_server *sv, const rc_request *req, int64_t *id) {
         return set_err(nullptr, RC_E_INVALID, "unknown table set");
     r->table_set = r->p.grey ? -1 : req->table_set;
     r->key = class_key(r->p, r->table_set);
+    {
+        // contexts are pooled per class and medium: a table set whose
+        // particles change starts a new class
+        auto it = sv->scatter.find(r->table_set);
+        if (it != sv->scatter.end()) r->scatter = it->second;
+        r->key += "/s" + std::to_string(sv->scatter_gen[r->table_set]);
+    }
     if ((double)context_bytes(r->p, std::max(r->photmax, kPilotPhotmax)) > sv->budget)
         return set_err(nullptr, RC_E_NOMEM, "request larger than the HBM budget");
     if (sv->stop) return set_err(nullptr, RC_E_STATE, "server is shutting down");

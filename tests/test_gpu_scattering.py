@@ -7,7 +7,8 @@ the cells of scattering events, final transmissivity, tally) and on every
 per-cell mean, variance and wall flux.  Covered: grey gas with forward
 scattering, narrow band with multigrid levels and both wall fluxes,
 specular y walls, the FP64 build, a batch that mixes a scattering and a
-non-scattering problem, and removing the scattering again.
+non-scattering problem, removing the scattering again, and served requests
+with particles per table set.
 """
 import numpy as np
 import pytest
@@ -149,3 +150,38 @@ def test_scattering_table_mismatch_is_rejected():
     with pytest.raises(RuntimeError):
         s.set_scattering(wrong)
     s.close()
+
+
+def test_served_requests_with_particles_equal_alone():
+    """The server takes particles per table set (and for grey requests):
+    requests solved in the mix equal the same solves alone, bit for bit; a
+    request submitted after the particles are removed solves without them
+    while the earlier ones keep theirs."""
+    p1, tabs, sc = _nb_case(photmax=32)
+    pg = W.channel_params(12, 8, 8, grey=True, photmax=32, nVar=2)
+    scg = api.Scattering.synthetic(nB=pg.grey_nB, nQ=1, nA=91, ksca_lo=0.8, ksca_hi=0.8, g_lo=0.5, g_hi=0.5)
+    T1, Tg = W.channel_field(p1, seed=21), W.channel_field(pg, seed=22)
+    s = api.Solver(p1, tabs)
+    plain = s.solve(T1, want64=False)
+    s.set_scattering(sc)
+    scat = s.solve(T1, want64=False)
+    s.close()
+    s = api.Solver(pg)
+    s.set_scattering(scg)
+    grey = s.solve(Tg, want64=False)
+    s.close()
+    assert not np.array_equal(plain.Q, scat.Q)
+    srv = api.Server(max_inflight=8)
+    ts = srv.add_tables(tabs)
+    srv.set_scattering(ts, sc)
+    srv.set_scattering(-1, scg)
+    a = srv.submit(p1, T1, table_set=ts)
+    g = srv.submit(pg, Tg)
+    srv.set_scattering(ts, None)
+    b = srv.submit(p1, T1, table_set=ts)
+    ra, rg, rb = srv.wait(a), srv.wait(g), srv.wait(b)
+    srv.close()
+    np.testing.assert_array_equal(ra.Q, scat.Q)
+    np.testing.assert_array_equal(ra.sigma, scat.sigma)
+    np.testing.assert_array_equal(rg.Q, grey.Q)
+    np.testing.assert_array_equal(rb.Q, plain.Q)
