@@ -26,11 +26,18 @@ Legs on one GPU (skipped with --no-legs):
   batched_small  the same with edges 16..32 and photmax 32/128;
   dns_source  the DNS coupling kernel (Q, sigma -> Qnew, Varnew, Knew,
          Gnew) on the 192x128x128 channel: device time per launch, HBM
-         roofline, host entry point time, CPU restatement time.
+         roofline, host entry point time, CPU restatement time;
+  batched_at_1pct, batched_small_at_1pct  the two mixes at equal 1%
+         relative std of max|Q| (photmax per problem from a pilot);
+  scattering  the benchmark solve with particle scattering added, next to
+         the same solve without particles;
+  serve  the open-loop serving stream below, capped in wall time.
 
 --serve runs the open-loop serving benchmark instead (Poisson arrivals at
 --load x measured capacity, tolerance-driven photmax, p50/p99 latency);
---precision runs the FP32-march vs FP64-build study at 192x128x128.
+--precision runs the FP32-march vs FP64-build study at 192x128x128;
+--dns-leg and --scatter-leg run one leg alone (profiling runs);
+--workload c4 runs the march on the precision study's 192x128x128 channel.
 
 --impl reference times the CPU restatement of the reference's ray loop
 (the reference has no CPU implementation of this path) on all host cores,
@@ -932,6 +939,8 @@ def main():
                     help="skip the 1%%-tolerance and batched-mix legs (profiling runs)")
     ap.add_argument("--serve", action="store_true", help="open-loop serving run instead of the solve benchmark")
     ap.add_argument("--precision", action="store_true", help="FP32 march vs FP64 build study instead")
+    ap.add_argument("--scatter-leg", dest="scatter_leg", action="store_true",
+                    help="only the particle-scattering leg (profiling runs; --photmax applies)")
     ap.add_argument("--dns-leg", dest="dns_leg", action="store_true",
                     help="only the DNS coupling leg (profiling runs)")
     ap.add_argument("--serve-requests", dest="serve_requests", type=int, default=200)
@@ -954,6 +963,14 @@ def main():
         run_serve(args, rank, local)
     elif args.precision:
         run_precision(args, rank, local)
+    elif args.scatter_leg:
+        import torch
+        torch.cuda.set_device(local)
+        flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda:%d" % local)
+        p, tabs, T, _ = workload(args.workload, args.photmax)
+        leg = leg_scattering(p, tabs, T, local, flush, steps=args.steps)
+        if rank == 0:
+            print(json.dumps(leg), flush=True)
     elif args.dns_leg:
         import torch
         torch.cuda.set_device(local)
