@@ -31,8 +31,9 @@ namespace rc {
 // start position is rebuilt from the emitting cell when a lane takes the
 // bundle) and two slot arrays; everything else stays in L1-cached global
 // memory, so that most of the SM's 256 KB of L1/shared storage caches the
-// temperature pyramid and the k / I_b tables (48-byte entries, the
-// round-1 layout, were 1.2% slower; 64-byte entries 4%).
+// temperature pyramid and the k / I_b tables (48-byte entries, an earlier
+// layout, were 1.2% slower; 64-byte entries 4%).  The scattering variant
+// keeps these entries and adds a small side array (see WarpShared).
 
 struct MarchArgs {
     const void *solves;          // DSolve<R>[nsolves] (run-time fields patched on the device)

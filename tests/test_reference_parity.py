@@ -13,8 +13,8 @@ Fixtures (tests/golden/make_ref_fixtures.py, built by oracle/ref_build.py):
                   rule corrected: west-wall flux.
 
 The reference draws cuRAND XORWOW, this solver Philox, so agreement is
-statistical; the criteria (tests/mc_stats.py) are the north star's "within 3
-combined standard deviations from nVar independent runs": per cell, the
+statistical; the criteria (tests/mc_stats.py) are the acceptance rule "within
+3 combined standard deviations from nVar independent runs": per cell, the
 count of |z| > 3 against its null distribution for 4-replicate sigmas; for
 aggregates (x planes, the wall mean), |z| < 3 at a family-wise error of
 0.27%.
