@@ -410,7 +410,7 @@ typedef struct rc_batch rc_batch;
  * nothing more. */
 int rc_batch_create(int device, int use_graph, rc_batch **out);
 int rc_batch_add(rc_batch *b, rc_ctx *ctx, const float *T_host, int zstart);
-int rc_batch_run(rc_batch *b);          /* enqueue; returns at once */
+int rc_batch_run(rc_batch *b);          /* enqueue (after the previous run of the batch has finished); returns at once */
 int rc_batch_wait(rc_batch *b, float *ms_device);
 /* Device time of the last run by phase: set-up of every member (field
  * copies, set-up kernels), the march, and tally plus result copies.  Waits

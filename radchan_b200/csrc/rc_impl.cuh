@@ -217,6 +217,10 @@ struct rc_ctx {
     float prio_thr = RC_PRIORITY_DEFAULT;  // long-ray priority: estimated path length in units of Lx (0: off)
     int num_sms = 148;
     bool has_tables = false;
+    // changes with every call that changes what a solve's descriptor holds
+    // (tables, particles, launch knobs): a batch captured before such a
+    // change is captured again
+    unsigned long long gen = 0;
     // DNS-coupling scratch (rc_dns_source): T1 pencil + four outputs, and a counter
     double *d_dns = nullptr;
     size_t dns_cap = 0;
@@ -554,6 +558,7 @@ struct Impl : ImplBase {
         if (!rc) rc = upload(d_wvc, wvc, err_);
         if (rc) return rc;
         c->has_tables = true;
+        c->gen++;
         return RC_OK;
     }
 
@@ -623,6 +628,7 @@ struct Impl : ImplBase {
         RC_CK(cudaMalloc((void **)&d_ki, ki.size() * sizeof(KIRow<R>)));
         RC_CK(cudaMemcpy(d_ki, ki.data(), ki.size() * sizeof(KIRow<R>), cudaMemcpyHostToDevice));
         c->has_tables = true;
+        c->gen++;
         return RC_OK;
     }
 
@@ -637,6 +643,7 @@ struct Impl : ImplBase {
         if (!s) {
             RC_CK(cudaDeviceSynchronize());
             release_scattering();
+            c->gen++;
             return RC_OK;
         }
         const int nBc = p.grey ? p.grey_nB : p.nB, nQc = p.grey ? 1 : p.nQ;
@@ -664,6 +671,7 @@ struct Impl : ImplBase {
             return rc;
         }
         nA = s->nA;
+        c->gen++;
         return RC_OK;
     }
 
@@ -1229,6 +1237,7 @@ struct Impl : ImplBase {
         c->block = bblock;
         c->minb = bminb;
         c->sort = bsort;
+        c->gen++;
         if (rpt_out) *rpt_out = brpt;
         if (block_out) *block_out = bblock;
         if (sort_out) *sort_out = bsort;

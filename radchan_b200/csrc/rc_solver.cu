@@ -277,6 +277,7 @@ int rc_set_launch(rc_ctx *c, int rays_per_thread, int block_threads, int sort_ba
         if (occupancy < 2 || occupancy > 4) return set_err(&c->err, RC_E_INVALID, "occupancy must be 2, 3 or 4");
         c->minb = occupancy;
     }
+    c->gen++;
     return RC_OK;
 }
 
@@ -366,6 +367,7 @@ struct rc_batch {
         rc_ctx *ctx;
         void *slot;
         int zstart;
+        unsigned long long gen;  // the context's generation the captured graph was built with
     };
     std::vector<Member> m;
     cudaStream_t st = nullptr;
@@ -619,6 +621,7 @@ int rc_batch_add(rc_batch *b, rc_ctx *c, const float *T_host, int zstart) {
         mm.ctx = c;
         mm.slot = s;
         mm.zstart = zstart;
+        mm.gen = c->gen;
         b->m.push_back(mm);
         return RC_OK;
     });
@@ -634,6 +637,16 @@ int rc_batch_run(rc_batch *b) {
     if (b->m.empty()) return set_err(&b->err, RC_E_STATE, "empty batch");
     cudaSetDevice(b->device);
     std::string *err_ = &b->err;
+    // the previous run reads the pinned descriptors and segment lists this
+    // run rewrites: it finishes first
+    RC_CK(cudaStreamSynchronize(b->st));
+    // a member whose tables, particles or launch knobs changed since the
+    // capture invalidates the graph (its descriptors and launch would be stale)
+    for (auto &mm : b->m)
+        if (mm.ctx->gen != mm.gen) {
+            mm.gen = mm.ctx->gen;
+            b->built = false;
+        }
     int rc = b->dbl ? batch_ensure_scratch<double>(b) : batch_ensure_scratch<float>(b);
     if (rc) return rc;
     // all allocations happen before any stream capture

@@ -185,3 +185,39 @@ def test_served_requests_with_particles_equal_alone():
     np.testing.assert_array_equal(ra.sigma, scat.sigma)
     np.testing.assert_array_equal(rg.Q, grey.Q)
     np.testing.assert_array_equal(rb.Q, plain.Q)
+
+
+def test_batch_follows_a_member_changed_after_capture():
+    """A batch captured into a CUDA graph is captured again when a member's
+    particles or launch knobs change afterwards (its descriptors would be
+    stale): each run equals the member solved alone as it is then."""
+    p1, tabs, sc = _nb_case(photmax=16)
+    T1 = W.channel_field(p1, seed=31)
+
+    def alone(scatter, rpt):
+        s = api.Solver(p1, tabs)
+        if scatter:
+            s.set_scattering(sc)
+        s.set_launch(rays_per_thread=rpt)
+        r = s.solve(T1)
+        s.close()
+        return r
+
+    s1 = api.Solver(p1, tabs)
+    rpt0 = s1.get_launch()[0]
+    b = api.Batch(use_graph=True)
+    b.add(s1, T1)
+    results = []
+    for change in (None, "particles", "knobs"):
+        if change == "particles":
+            s1.set_scattering(sc)
+        elif change == "knobs":
+            s1.set_launch(rays_per_thread=2 * rpt0)
+        b.run()
+        b.wait()
+        results.append(b.collect(0))
+    b.close()
+    s1.close()
+    for r, (scatter, rpt) in zip(results, ((False, rpt0), (True, rpt0), (True, 2 * rpt0))):
+        a = alone(scatter, rpt)
+        _equal(r, dict(q64=a.q64, var64=a.var64, qw64=a.qw64, vw64=a.vw64))
