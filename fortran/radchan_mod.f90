@@ -54,6 +54,12 @@ module radchan_mod
     type(c_ptr) :: Tnb, kP, wvl, wvr, wvc, kavg, kq, prob, probg, wq
   end type rc_tables
 
+  ! mirror of struct rc_scattering (borrowed pointers into a particle set)
+  type, bind(C), public :: rc_scattering
+    integer(c_int) :: nB, nQ, nA
+    type(c_ptr) :: ksca, kabs, theta, phase_cdf
+  end type rc_scattering
+
   ! mirror of struct rc_dns_coupling: what the DNS does with a finished
   ! solve (channel.f:249-266, fixvar.f:16-43 and :179-242)
   type, bind(C), public :: rc_dns_coupling
@@ -67,6 +73,7 @@ module radchan_mod
   public :: rc_params_from_headers, rc_create, rc_set_tables, rc_tables_read_dir, rc_tables_view
   public :: rc_tables_free, rc_solve_async, rc_collect, rc_destroy, rc_last_error
   public :: rc_legacy_configure, rc_dns_source, rc_legacy_source, c_string
+  public :: rc_scattering_read_dir, rc_scattering_view, rc_scattering_free, rc_set_scattering
 
   interface
     ! the reference's entry points (mc_gpu_noint.cu:660, :876)
@@ -118,6 +125,32 @@ module radchan_mod
       type(c_ptr), value :: ctx
       type(rc_tables), intent(in) :: t
     end function rc_set_tables
+
+    ! particles of the table generator's files (particles/NarrBand%d.txt,
+    ! particles/prob_scatt.txt) for the context's later solves
+    integer(c_int) function rc_scattering_read_dir(dir, nB, nQ, ps) bind(C, name="rc_scattering_read_dir")
+      import :: c_char, c_int, c_ptr
+      character(kind=c_char), intent(in) :: dir(*)
+      integer(c_int), value :: nB, nQ
+      type(c_ptr), intent(out) :: ps
+    end function rc_scattering_read_dir
+
+    integer(c_int) function rc_scattering_view(ps, view) bind(C, name="rc_scattering_view")
+      import :: c_int, c_ptr, rc_scattering
+      type(c_ptr), value :: ps
+      type(rc_scattering), intent(out) :: view
+    end function rc_scattering_view
+
+    subroutine rc_scattering_free(ps) bind(C, name="rc_scattering_free")
+      import :: c_ptr
+      type(c_ptr), value :: ps
+    end subroutine rc_scattering_free
+
+    integer(c_int) function rc_set_scattering(ctx, s) bind(C, name="rc_set_scattering")
+      import :: c_int, c_ptr, rc_scattering
+      type(c_ptr), value :: ctx
+      type(rc_scattering), intent(in) :: s
+    end function rc_set_scattering
 
     integer(c_int) function rc_solve_async(ctx, T, zstart, ticket) bind(C, name="rc_solve_async")
       import :: c_float, c_int, c_int32_t, c_ptr

@@ -143,3 +143,37 @@ def test_create_without_gpu_reports_error():
     p = api.default_params()
     with pytest.raises(L.RadChanError):
         api.Solver(p)
+
+
+def test_fortran_module_binds_declared_symbols_and_mirrors_structs():
+    """fortran/radchan_mod.f90 (no Fortran compiler here): every bind(C)
+    name is a function the header declares and the library exports, and
+    each bind(C) derived type lists as many components as the C struct it
+    mirrors."""
+    src = open(os.path.join(ROOT, "fortran", "radchan_mod.f90")).read()
+    names = re.findall(r'bind\(C,\s*name="(\w+)"\)', src)
+    declared = set(_header_functions(os.path.join(ROOT, "include", "radchan.h")))
+    lib = L.lib()
+    assert len(names) >= 15
+    for n in names:
+        assert n in declared, n
+        assert hasattr(lib, n), n
+    hdr = re.sub(r"/\*.*?\*/", "", open(os.path.join(ROOT, "include", "radchan.h")).read(), flags=re.S)
+    for tname in ("rc_params", "rc_tables", "rc_scattering", "rc_dns_coupling"):
+        body = re.search(r"type, bind\(C\), public :: %s\n(.*?)end type %s" % (tname, tname), src, flags=re.S).group(1)
+        f_fields = []
+        for line in body.splitlines():
+            line = line.split("!")[0]
+            if "::" not in line:
+                continue
+            decl = line.split("::")[1]
+            f_fields += [x.strip().split("(")[0] for x in re.split(r",(?![^()]*\))", decl) if x.strip()]
+        cbody = re.search(r"typedef struct %s \{(.*?)\} %s;" % (tname, tname), hdr, flags=re.S).group(1)
+        c_fields = []
+        for stmt in cbody.split(";"):
+            stmt = stmt.strip()
+            if not stmt:
+                continue
+            decl = re.sub(r"^(const\s+)?(unsigned\s+)?\w+\s*\**", "", stmt)
+            c_fields += [re.sub(r"[\s\*]|\[.*?\]", "", x) for x in decl.split(",") if x.strip()]
+        assert [f.lower() for f in f_fields] == [c.lower() for c in c_fields], (tname, f_fields, c_fields)
