@@ -137,6 +137,11 @@ struct rc_server {
     cudaEvent_t mend[kNQ] = {};      // march of the parity's latest quantum done
     bool q_used[kNQ] = {};
     int q_par = 0, last_par = -1;
+    // the set-up chains of the requests a quantum starts run side by side on
+    // these streams, forked from and joined back into the quantum's stream
+    static constexpr int kSide = 16;
+    cudaStream_t side[kSide] = {};
+    cudaEvent_t fork = nullptr, join[kSide] = {};
     double busy_since = -1.0;
     std::string err;
 };
@@ -619,12 +624,27 @@ void worker_loop(rc_server *sv) {
                 for (SrvReq *r : sv->running)
                     if (r->stage < ST_DONE && r->phase != PH_TALLY) fail(sv, r, rc, sv->err);
             } else {
-                if (prepare)
-                    for (SrvReq *r : sv->running) {
-                        if (r->stage >= ST_DONE || r->phase != PH_PREPARE) continue;
-                        const int e = start_stage(sv, r, st);
+                if (prepare) {
+                    // each starting request's field copy and set-up kernels
+                    // form a chain of their own, forked round-robin over the
+                    // side streams and joined before the quantum's march
+                    std::vector<SrvReq *> starting;
+                    for (SrvReq *r : sv->running)
+                        if (r->stage < ST_DONE && r->phase == PH_PREPARE) starting.push_back(r);
+                    const int ns = std::min<int>((int)starting.size(), rc_server::kSide);
+                    bool forked = cudaEventRecord(sv->fork, st) == cudaSuccess;
+                    for (int k = 0; k < ns && forked; ++k)
+                        forked = cudaStreamWaitEvent(sv->side[k], sv->fork, 0) == cudaSuccess;
+                    for (size_t i = 0; i < starting.size(); ++i) {
+                        SrvReq *r = starting[i];
+                        const int e = start_stage(sv, r, forked ? sv->side[i % ns] : st);
                         if (e) fail(sv, r, e, r->ctx ? r->ctx->err : g_err);
                     }
+                    for (int k = 0; k < ns && forked; ++k) {
+                        cudaEventRecord(sv->join[k], sv->side[k]);
+                        cudaStreamWaitEvent(st, sv->join[k], 0);
+                    }
+                }
                 for (SrvReq *r : sv->running)
                     if (r->stage < ST_DONE && r->phase == PH_MARCH) marching.push_back(r);
                 if (!marching.empty()) {
@@ -706,6 +726,10 @@ int rc_server_create(int device, double hbm_budget_bytes, int max_inflight, rc_s
              cudaMalloc((void **)&sv->d_counter[i], sizeof(unsigned long long)) == cudaSuccess &&
              cudaEventCreateWithFlags(&sv->pre_done[i], cudaEventDisableTiming) == cudaSuccess &&
              cudaEventCreateWithFlags(&sv->mend[i], cudaEventDisableTiming) == cudaSuccess;
+    ok = ok && cudaEventCreateWithFlags(&sv->fork, cudaEventDisableTiming) == cudaSuccess;
+    for (int i = 0; i < rc_server::kSide && ok; ++i)
+        ok = cudaStreamCreateWithFlags(&sv->side[i], cudaStreamNonBlocking) == cudaSuccess &&
+             cudaEventCreateWithFlags(&sv->join[i], cudaEventDisableTiming) == cudaSuccess;
     if (!ok) {
         rc_server_destroy(sv);
         return set_err(nullptr, RC_E_CUDA, "server stream/event creation failed");
@@ -900,6 +924,14 @@ int rc_server_destroy(rc_server *sv) {
         if (sv->mend[i]) cudaEventDestroy(sv->mend[i]);
         if (sv->qst[i]) cudaStreamDestroy(sv->qst[i]);
     }
+    for (int i = 0; i < rc_server::kSide; ++i) {
+        if (sv->side[i]) {
+            cudaStreamSynchronize(sv->side[i]);
+            cudaStreamDestroy(sv->side[i]);
+        }
+        if (sv->join[i]) cudaEventDestroy(sv->join[i]);
+    }
+    if (sv->fork) cudaEventDestroy(sv->fork);
     if (sv->st) cudaStreamDestroy(sv->st);
     delete sv;
     return RC_OK;
