@@ -74,6 +74,8 @@ module radchan_mod
   public :: rc_tables_free, rc_solve_async, rc_collect, rc_destroy, rc_last_error
   public :: rc_legacy_configure, rc_dns_source, rc_legacy_source, c_string
   public :: rc_scattering_read_dir, rc_scattering_view, rc_scattering_free, rc_set_scattering
+  public :: rc_slab_range, rc_slab_unique_id, rc_slab_comm_create, rc_slab_solve, rc_slab_last_error
+  public :: rc_slab_comm_destroy
 
   interface
     ! the reference's entry points (mc_gpu_noint.cu:660, :876)
@@ -180,6 +182,49 @@ module radchan_mod
       character(kind=c_char), intent(out) :: buf(*)
       integer(c_size_t), value :: len
     end function rc_last_error
+
+    ! one solve over several GPUs by z slabs (NCCL inside the library):
+    ! rank 0 makes the group id, MPI_Bcast hands its 128 bytes to every
+    ! rank, each rank joins with its GPU and solves with a context created
+    ! with p_col = nranks; every rank receives the whole solution
+    integer(c_int) function rc_slab_range(kmax, nranks, rank, kloc, zstart) bind(C, name="rc_slab_range")
+      import :: c_int
+      integer(c_int), value :: kmax, nranks, rank
+      integer(c_int), intent(out) :: kloc, zstart
+    end function rc_slab_range
+
+    integer(c_int) function rc_slab_unique_id(id) bind(C, name="rc_slab_unique_id")
+      import :: c_int, c_int8_t
+      integer(c_int8_t), intent(out) :: id(128)
+    end function rc_slab_unique_id
+
+    integer(c_int) function rc_slab_comm_create(device, nranks, rank, id, timeout_s, comm) &
+        bind(C, name="rc_slab_comm_create")
+      import :: c_double, c_int, c_int8_t, c_ptr
+      integer(c_int), value :: device, nranks, rank
+      integer(c_int8_t), intent(in) :: id(128)
+      real(c_double), value :: timeout_s
+      type(c_ptr), intent(out) :: comm
+    end function rc_slab_comm_create
+
+    ! T (whole field, real(4)), q64, var64 (real(8), imax*jmax*kmax), qw64,
+    ! vw64 (real(8), 2*jmax*kmax, or c_null_ptr): c_loc of host or device arrays
+    integer(c_int) function rc_slab_solve(comm, ctx, T, q64, var64, qw64, vw64) bind(C, name="rc_slab_solve")
+      import :: c_int, c_ptr
+      type(c_ptr), value :: comm, ctx, T, q64, var64, qw64, vw64
+    end function rc_slab_solve
+
+    integer(c_int) function rc_slab_last_error(comm, buf, len) bind(C, name="rc_slab_last_error")
+      import :: c_char, c_int, c_ptr, c_size_t
+      type(c_ptr), value :: comm
+      character(kind=c_char), intent(out) :: buf(*)
+      integer(c_size_t), value :: len
+    end function rc_slab_last_error
+
+    integer(c_int) function rc_slab_comm_destroy(comm) bind(C, name="rc_slab_comm_destroy")
+      import :: c_int, c_ptr
+      type(c_ptr), value :: comm
+    end function rc_slab_comm_destroy
 
     ! tables: c_null_ptr in grey mode, else c_loc of an rc_tables view
     integer(c_int) function rc_legacy_configure(p, tables) bind(C, name="rc_legacy_configure")

@@ -57,6 +57,7 @@ extern "C" {
 #define RC_E_BUSY       -7   /* no free slot / queue full */
 #define RC_E_NOTFOUND   -8
 #define RC_E_CANCELLED  -9   /* a served request was cancelled */
+#define RC_E_TIMEOUT   -10   /* a multi-GPU group did not form or a collective did not finish in time */
 
 /* wall indices: west (x=0), east (x=Lx), south (y=0), north (y=Ly),
  * bottom (z=0), top (z=Lz) -- the order of param.h:68-100 */
@@ -343,6 +344,9 @@ int rc_autotune(rc_ctx *ctx, const float *T, int zstart, int pilot_photmax,
 int rc_solve_noalloc(rc_ctx *ctx, const float *T_dev, int zstart, double *q64_dev, double *var64_dev,
                      double *qw64_dev, double *vw64_dev);
 int rc_destroy(rc_ctx *ctx);
+/* The parameters a context was created with and its device (either output
+ * may be NULL). */
+int rc_get_params(const rc_ctx *ctx, rc_params *p, int *device);
 int rc_last_error(const rc_ctx *ctx, char *buf, size_t len);
 /* Failure injection for tests of the error paths (no counterpart in the
  * reference): the next `count` times the named host-side site is reached
@@ -396,6 +400,59 @@ int rc_sample_bands(rc_ctx *ctx, rc_ticket ticket, int kind, int n, const float 
  * solve's temperature pyramid and tables it is the ceiling of the march's
  * gathers, which stay L2-resident. */
 int rc_probe_gather(int device, size_t bytes, int mode, int iters, double *sectors_per_s, float *ms_best);
+
+/* ---------------- one solve over several GPUs (NCCL) ---------------- */
+
+/* The reference spreads one solve over GPUs and nodes by z slabs of the
+ * emitting cells while every GPU holds the whole field (mc_gpu_noint.cu:
+ * 95-98: kloc = kmax/p_col planes from zstart), and the DNS combines the
+ * slabs' results over MPI (fixvar.f:202-203).  These calls do the same from
+ * C over NCCL, one process (or thread) per GPU: rank r of a group of N
+ * solves the planes rc_slab_range names, of the field that rank 0 holds,
+ * and every rank ends with the whole solution.  Bundles draw from counters
+ * of the global cell index, so the gathered solution equals the one-GPU
+ * solve of the same problem bit for bit.  NCCL is loaded when the first id
+ * or communicator is made (libnccl.so.2, or the file RC_NCCL_LIBRARY
+ * names); the rest of the library does not need it.  There is no other
+ * data-path collective: the field is broadcast once and the results are
+ * all-gathered once per solve. */
+#define RC_SLAB_ID_BYTES 128   /* NCCL_UNIQUE_ID_BYTES */
+typedef struct rc_slab_comm rc_slab_comm;
+/* Planes of rank `rank` in a group of `nranks`: kloc = kmax/nranks planes
+ * starting at the 1-based zstart = rank*kloc + 1 (kmax must be a multiple
+ * of nranks, as p_col requires in the reference). */
+int rc_slab_range(int kmax, int nranks, int rank, int *kloc, int *zstart);
+/* A new group id, made on one rank; every rank passes the same
+ * RC_SLAB_ID_BYTES bytes to rc_slab_comm_create (e.g. after MPI_Bcast). */
+int rc_slab_unique_id(void *id);
+/* Joins group `id` as rank `rank` of `nranks` on `device`.  Returns once
+ * every rank has joined; after timeout_s seconds (<= 0: 300) without that,
+ * RC_E_TIMEOUT and the group is abandoned.  The same timeout bounds every
+ * later collective of the communicator: one that does not finish in time
+ * aborts the group (RC_E_TIMEOUT; the communicator is then unusable and
+ * only rc_slab_comm_destroy is valid). */
+int rc_slab_comm_create(int device, int nranks, int rank, const void *id, double timeout_s,
+                        rc_slab_comm **out);
+/* One solve of ctx's problem over the group.  Every rank calls it with a
+ * context of the same problem created with p_col = nranks on the
+ * communicator's device (tables and launch knobs set alike).  T: the whole
+ * field (kmax+2, jmax+2, imax+2) on every rank; rank 0's is broadcast into
+ * the others' (their contents are overwritten).  q64/var64
+ * [kmax][jmax][imax] (required) and qw64/vw64 [2][kmax][jmax] (optional)
+ * receive the whole solution in the compact layouts of rc_collect on every
+ * rank.  Each array may be device memory (used in place) or host memory
+ * (staged through device buffers the communicator keeps).  Returns when
+ * the results are in place.  A solve error on one rank (RC_E_RANGE for a
+ * non-finite field, which every rank sees) is returned after the
+ * collectives, so the ranks stay in step; an argument error is returned
+ * before them, and the other ranks' collectives then end by the timeout. */
+int rc_slab_solve(rc_slab_comm *comm, rc_ctx *ctx, float *T, double *q64, double *var64, double *qw64,
+                  double *vw64);
+/* Message of the communicator's last failure. */
+int rc_slab_last_error(const rc_slab_comm *comm, char *buf, size_t len);
+/* Leaves the group (collective over the ranks of a healthy group; a group
+ * that timed out is aborted instead) and frees the communicator. */
+int rc_slab_comm_destroy(rc_slab_comm *comm);
 
 /* ---------------- batched solves ---------------- */
 

@@ -16,7 +16,8 @@ LIB_PATH = os.path.join(HERE, "libradchan_checked.so" if os.environ.get("RADCHAN
 RC_MAX_LEVELS = 9
 RC_OK = 0
 RC_E = {-1: "RC_E_INVALID", -2: "RC_E_CUDA", -3: "RC_E_NOMEM", -4: "RC_E_IO", -5: "RC_E_STATE",
-        -6: "RC_E_RANGE", -7: "RC_E_BUSY", -8: "RC_E_NOTFOUND", -9: "RC_E_CANCELLED"}
+        -6: "RC_E_RANGE", -7: "RC_E_BUSY", -8: "RC_E_NOTFOUND", -9: "RC_E_CANCELLED",
+        -10: "RC_E_TIMEOUT"}
 RC_WEST, RC_EAST, RC_SOUTH, RC_NORTH, RC_BOT, RC_TOP = range(6)
 
 
@@ -148,6 +149,13 @@ _SIGS = [
                          C.POINTER(C.c_int)]),
     ("rc_solve_noalloc", _I, [_VP, _VP, _I, _VP, _VP, _VP, _VP]),
     ("rc_destroy", _I, [_VP]),
+    ("rc_get_params", _I, [_VP, C.POINTER(RcParams), C.POINTER(C.c_int)]),
+    ("rc_slab_range", _I, [_I, _I, _I, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+    ("rc_slab_unique_id", _I, [C.c_char_p]),
+    ("rc_slab_comm_create", _I, [_I, _I, _I, C.c_char_p, C.c_double, C.POINTER(_VP)]),
+    ("rc_slab_solve", _I, [_VP, _VP, _VP, _VP, _VP, _VP, _VP]),
+    ("rc_slab_last_error", _I, [_VP, C.c_char_p, C.c_size_t]),
+    ("rc_slab_comm_destroy", _I, [_VP]),
     ("rc_last_error", _I, [_VP, C.c_char_p, C.c_size_t]),
     ("rc_debug_fail_next", _I, [C.c_char_p, _I]),
     ("rc_grid_level", _I, [C.POINTER(RcParams), _I, _FP, _FP, _FP, _FP, _FP, _FP]),
@@ -218,4 +226,13 @@ class RadChanError(RuntimeError):
 def check(rc, ctx=None):
     if rc != RC_OK:
         raise RadChanError(rc, last_error(ctx))
+    return rc
+
+
+def check_slab(rc, comm=None):
+    """check() for the rc_slab_* calls (messages kept per communicator)."""
+    if rc != RC_OK:
+        buf = C.create_string_buffer(1024)
+        lib().rc_slab_last_error(comm, buf, 1024)
+        raise RadChanError(rc, buf.value.decode(errors="replace"))
     return rc

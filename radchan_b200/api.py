@@ -448,6 +448,62 @@ class Solver:
             pass
 
 
+def slab_range(kmax: int, nranks: int, rank: int):
+    """rc_slab_range: (kloc, zstart) of rank `rank` in a group of `nranks`."""
+    kl, zs = C.c_int(), C.c_int()
+    L.check(L.lib().rc_slab_range(kmax, nranks, rank, C.byref(kl), C.byref(zs)))
+    return kl.value, zs.value
+
+
+def slab_unique_id() -> bytes:
+    """rc_slab_unique_id: a new group id (RC_SLAB_ID_BYTES bytes) for
+    SlabComm; made on one rank and handed to the others."""
+    buf = C.create_string_buffer(128)
+    L.check_slab(L.lib().rc_slab_unique_id(buf))
+    return buf.raw
+
+
+class SlabComm:
+    """One rank of a group that solves problems by z slabs over NCCL from
+    the library itself (rc_slab_comm_create .. rc_slab_comm_destroy): the
+    C route to what ShardedSolver does over torch.distributed."""
+
+    def __init__(self, device: int, nranks: int, rank: int, uid: bytes, timeout_s: float = 300.0):
+        if len(uid) != 128:
+            raise ValueError("a group id has 128 bytes")
+        self.comm = C.c_void_p()
+        L.check_slab(L.lib().rc_slab_comm_create(device, nranks, rank, uid, float(timeout_s), C.byref(self.comm)))
+        self.nranks, self.rank = nranks, rank
+
+    def solve(self, solver: "Solver", T: int, q64: int, var64: int, qw64: int = 0, vw64: int = 0):
+        """rc_slab_solve with pointers to device or host arrays (0 skips a
+        wall output): the whole solution on every rank."""
+        v = lambda x: C.c_void_p(x) if x else None
+        L.check_slab(L.lib().rc_slab_solve(self.comm, solver.ctx, v(T), v(q64), v(var64), v(qw64), v(vw64)),
+                     self.comm)
+
+    def solve_arrays(self, solver: "Solver", T=None):
+        """rc_slab_solve with numpy arrays in host memory: T the whole field
+        (read on rank 0); returns (q64, var64, qw64, vw64) of the whole
+        problem."""
+        p = solver.p
+        shape = field_shape(p)
+        T = np.zeros(shape, np.float32) if T is None else np.ascontiguousarray(T, dtype=np.float32).copy()
+        if T.shape != shape:
+            raise ValueError("T has shape %s, expected %s" % (T.shape, shape))
+        q = np.empty((p.kmax, p.jmax, p.imax))
+        v = np.empty_like(q)
+        qw = np.empty((2, p.kmax, p.jmax))
+        vw = np.empty_like(qw)
+        self.solve(solver, T.ctypes.data, q.ctypes.data, v.ctypes.data, qw.ctypes.data, vw.ctypes.data)
+        return q, v, qw, vw
+
+    def close(self):
+        if self.comm:
+            L.check_slab(L.lib().rc_slab_comm_destroy(self.comm))
+            self.comm = None
+
+
 class Batch:
     """Many solves of uneven size in one persistent launch (rc_batch_*)."""
 

@@ -77,7 +77,7 @@ def build(verbose: bool = False, ptxas_verbose: bool = False, checked: bool = Fa
             if log:
                 sys.stderr.write(log)
     if not os.path.exists(lib) or os.path.getmtime(lib) < max(os.path.getmtime(o) for o in objs):
-        cmd = [NVCC] + ARCH + ["-shared", "-o", lib] + objs + ["-lpthread"]
+        cmd = [NVCC] + ARCH + ["-shared", "-o", lib] + objs + ["-lpthread", "-ldl"]
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError("link failed:\n%s\n%s" % (" ".join(cmd), r.stderr))

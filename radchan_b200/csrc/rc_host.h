@@ -7,6 +7,17 @@
 #include <vector>
 #include "radchan.h"
 
+namespace rc_detail {
+// message of the last failure of a context-free call (per host thread)
+inline thread_local std::string g_err;
+
+inline int set_err(std::string *dst, int code, const std::string &m) {
+    if (dst) *dst = m;
+    g_err = m;
+    return code;
+}
+}  // namespace rc_detail
+
 namespace rc {
 
 // Wall treatment used by the march; derived from param.h bd* and the

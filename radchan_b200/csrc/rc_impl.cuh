@@ -32,14 +32,6 @@
 using namespace rc;
 
 namespace rc_detail {
-// message of the last failure of a context-free call (per host thread)
-inline thread_local std::string g_err;
-
-inline int set_err(std::string *dst, int code, const std::string &m) {
-    if (dst) *dst = m;
-    g_err = m;
-    return code;
-}
 
 // Host-side failure injection (rc_debug_fail_next): a named site reached
 // while armed fails as if its CUDA call had returned an error, without

@@ -326,6 +326,13 @@ int rc_destroy(rc_ctx *c) {
     return RC_OK;
 }
 
+int rc_get_params(const rc_ctx *c, rc_params *p, int *device) {
+    if (!c) return set_err(nullptr, RC_E_INVALID, "NULL context");
+    if (p) *p = c->p;
+    if (device) *device = c->device;
+    return RC_OK;
+}
+
 int rc_last_error(const rc_ctx *c, char *buf, size_t len) {
     const std::string &m = c ? c->err : g_err;
     if (buf && len) snprintf(buf, len, "%s", m.c_str());

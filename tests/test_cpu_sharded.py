@@ -113,3 +113,54 @@ def test_fortran_layout_of_a_gathered_result():
     np.testing.assert_array_equal(Q[1:-1, 1:-1, 0], r.qw64[0].astype(np.float32))
     assert np.all(Q[1:-1, 1:-1, -1] == 0)   # east flux not computed
     assert np.all(Q[0] == 0) and np.all(Q[:, 0] == 0)
+
+
+# ---- the same decomposition behind the C ABI (rc_slab_*, NCCL loaded by the
+#      library): what runs without a GPU
+
+def test_native_slab_range_matches_the_python_decomposition():
+    for kmax in (1, 6, 64, 2304):
+        for ws in (1, 2, 3, 4, 8):
+            for rank in range(ws):
+                if kmax % ws:
+                    with pytest.raises(api.L.RadChanError):
+                        api.slab_range(kmax, ws, rank)
+                else:
+                    assert api.slab_range(kmax, ws, rank) == sharded.slab(kmax, ws, rank)
+    for bad in ((64, 4, 4), (64, 0, 0), (64, 2, -1), (0, 1, 0)):
+        with pytest.raises(api.L.RadChanError) as e:
+            api.slab_range(*bad)
+        assert e.value.code == -1
+
+
+def test_native_slab_group_ids_and_argument_checks():
+    import ctypes as C
+    a, b = api.slab_unique_id(), api.slab_unique_id()
+    assert len(a) == 128 and a != b
+    lib = api.L.lib()
+    comm = C.c_void_p()
+    assert lib.rc_slab_comm_create(0, 0, 0, a, 1.0, C.byref(comm)) == -1
+    assert lib.rc_slab_comm_create(0, 2, 2, a, 1.0, C.byref(comm)) == -1
+    assert lib.rc_slab_comm_create(0, 1, 0, None, 1.0, C.byref(comm)) == -1
+    assert not comm.value
+    assert lib.rc_slab_solve(None, None, None, None, None, None, None) == -1
+    assert lib.rc_slab_comm_destroy(None) == 0
+
+
+def test_native_slab_reports_a_missing_nccl():
+    """Without an NCCL to load, the group calls fail with RC_E_NOTFOUND and
+    say which file was tried (the rest of the library works without it)."""
+    import subprocess
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    code = ("from radchan_b200 import api\n"
+            "try:\n"
+            "    api.slab_unique_id()\n"
+            "except api.L.RadChanError as e:\n"
+            "    assert e.code == -8 and 'cannot load NCCL' in str(e) and 'no_such_nccl' in str(e), str(e)\n"
+            "    print('refused')\n"
+            "print(api.slab_range(8, 2, 1))\n")
+    env = dict(os.environ, RC_NCCL_LIBRARY="/nonexistent/no_such_nccl.so")
+    r = subprocess.run([sys.executable, "-c", code], cwd=root, env=env, capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    assert r.stdout.split() == ["refused", "(4,", "5)"]
