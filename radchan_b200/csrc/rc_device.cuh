@@ -41,6 +41,7 @@ constexpr int kRing = 64;    // per-warp ring of emitted bundles (two waves)
 constexpr int kGuide = 256;  // buckets of the band-CDF guide tables
 constexpr int kFeedIdle = 14; // idle lanes that make a warp leave its step loop to take new bundles
 constexpr int kChunkMax = 8;  // tiles a warp claims per work-queue fetch (guided: fewer near the end)
+constexpr int kPhaseGuide = 64;  // phase-CDF guide buckets per band (scattering turns)
 
 // ---------------------------------------------------------------------------
 // descriptors
@@ -117,6 +118,7 @@ struct DSolve {
     const R *ksca;            // [nB][nQ] scattering coefficient (scaled by chanHeight)
     const R *pcdf;            // [nB][nA] cumulative phase-function probability, last = 1
     const R *pth;             // [nA] scattering angles in turns (theta / 2 pi)
+    const uint16_t *pguide;   // [nB][kPhaseGuide+1] phase-CDF search brackets (phase_index)
     int nA;
     int pad3;
     DScalars *sc;
@@ -580,19 +582,37 @@ __device__ __forceinline__ R scatter_first_dist(const DSolve<R> &S, uint4 ctr, R
     return dist;
 }
 
+// Angle index of a uniform u on the phase CDF of a band: the first a in
+// [1, nA-1] with u < cdf[a] (nA-1 if none), which is what a bisection over
+// the whole table returns for a CDF that starts at 0 and does not decrease.
+// guide[q] (q = 0..kPhaseGuide) is the first a >= 1 with cdf[a] > q /
+// kPhaseGuide (nA-1 if none), so for u in bucket q the answer lies in
+// (guide[q] - 1, guide[q+1]] and the bisection runs over that bracket only:
+// one or two table reads instead of log2(nA) dependent ones.
+template <typename R>
+__device__ __forceinline__ int phase_index(const R *cdf, const uint16_t *guide, R u) {
+    const int q = min((int)(u * (R)kPhaseGuide), kPhaseGuide - 1);
+    int lo = (int)guide[q] - 1, hi = (int)guide[q + 1];
+    while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (u < cdf[mid]) hi = mid;
+        else lo = mid;
+    }
+    return hi;
+}
+
 // New direction of a bundle travelling along (sx, sy, sz) in band nb at a
 // scattering event (ctr: its counter words x, y, z and the number of the
 // event in w; ks > 0 its scattering coefficient), with the reciprocals of
 // the new direction and the free path to the event after it.  Everything is
-// passed and returned by value: the function is not inlined (it is rare and
-// long), and a reference would oblige the caller to keep the ray in local
-// memory.
+// passed and returned by value: a reference would oblige the caller to keep
+// the ray in local memory.
 template <typename R>
 struct TurnOut {
     R sx, sy, sz, isx, isy, isz, dist;
 };
 template <typename R>
-__device__ __noinline__ TurnOut<R> scatter_turn_v(R sx, R sy, R sz, int nb, uint4 ctr, R ks, const DSolve<R> *Sp) {
+__device__ __forceinline__ TurnOut<R> scatter_turn_v(R sx, R sy, R sz, int nb, uint4 ctr, R ks, const DSolve<R> *Sp) {
     const DSolve<R> &S = *Sp;
     rc_u32x4 c;
     c.x = ctr.x;
@@ -603,12 +623,8 @@ __device__ __noinline__ TurnOut<R> scatter_turn_v(R sx, R sy, R sz, int nb, uint
     const R u_t = (R)rc_u01(d.x), u_p = (R)rc_u01(d.y), u_s = (R)rc_u01(d.z);
     const int nA = S.nA;
     const R *cdf = S.pcdf + RC_IX((size_t)nb * nA, (long long)S.nB * nA, SITE_PHASE, S);
-    int lo = 0, hi = nA - 1;
-    while (hi - lo > 1) {
-        const int mid = (lo + hi) >> 1;
-        if (u_t < cdf[mid]) hi = mid;
-        else lo = mid;
-    }
+    const int hi = phase_index(cdf, S.pguide + RC_IX((size_t)nb * (kPhaseGuide + 1),
+                                                     (long long)S.nB * (kPhaseGuide + 1), SITE_PHASE, S), u_t);
     const R c0 = cdf[hi - 1], c1 = cdf[hi];
     R fr = (c1 > c0) ? (u_t - c0) / (c1 - c0) : (R)0;
     if (fr > (R)1) fr = (R)1;

@@ -254,6 +254,7 @@ struct Impl : ImplBase {
     int nT = 0, nB = 0, nQ = 0;
     // scattering particles (rc_set_scattering): coefficient, phase CDF, angles in turns
     R *d_ksca = nullptr, *d_pcdf = nullptr, *d_pth = nullptr;
+    uint16_t *d_pguide = nullptr;
     int nA = 0;
     std::vector<Slot<R>> slots;
     int smem_opt_in = 0;
@@ -291,6 +292,7 @@ struct Impl : ImplBase {
         dfree(d_ksca);
         dfree(d_pcdf);
         dfree(d_pth);
+        dfree(d_pguide);
         nA = 0;
     }
 
@@ -654,10 +656,28 @@ struct Impl : ImplBase {
             for (int a = 0; a < s->nA; ++a)
                 cdf[(size_t)b * s->nA + a] = (a == s->nA - 1) ? 1.0f : s->phase_cdf[(size_t)b * s->nA + a];
         for (int a = 0; a < s->nA; ++a) th[a] = rc_angle_turns(s->theta[a]);
+        // search brackets of the phase CDF (phase_index): guide[q] is the
+        // first angle a >= 1 with cdf[a] > q / kPhaseGuide, nA-1 if none
+        std::vector<uint16_t> guide((size_t)s->nB * (kPhaseGuide + 1));
+        for (int b = 0; b < s->nB; ++b) {
+            const float *cb = &cdf[(size_t)b * s->nA];
+            int a = 1;
+            for (int q = 0; q <= kPhaseGuide; ++q) {
+                const float thr = (float)q / (float)kPhaseGuide;
+                while (a < s->nA - 1 && !(cb[a] > thr)) ++a;
+                guide[(size_t)b * (kPhaseGuide + 1) + q] = (uint16_t)a;
+            }
+        }
         release_scattering();
         int rc = upload(d_ksca, ks, err_);
         if (!rc) rc = upload(d_pcdf, cdf, err_);
         if (!rc) rc = upload(d_pth, th, err_);
+        if (!rc) {
+            cudaError_t e = cudaMalloc((void **)&d_pguide, guide.size() * sizeof(uint16_t));
+            if (e == cudaSuccess)
+                e = cudaMemcpy(d_pguide, guide.data(), guide.size() * sizeof(uint16_t), cudaMemcpyHostToDevice);
+            if (e != cudaSuccess) rc = set_err(err_, RC_E_CUDA, std::string("phase guide: ") + cudaGetErrorString(e));
+        }
         if (rc) {
             release_scattering();
             return rc;
@@ -755,6 +775,7 @@ struct Impl : ImplBase {
         d.ksca = d_ksca;
         d.pcdf = d_pcdf;
         d.pth = d_pth;
+        d.pguide = d_pguide;
         d.nA = nA;
         d.probq = d_probq;
         d.Ibw = d_Ibw;

@@ -198,7 +198,7 @@ __global__ void __launch_bounds__(256, MINB) k_march(MarchArgs a) {
     unsigned amask = 0u, p1mask = 0u;
     // lane state
     bool active = false;
-    int myb = 0, mypar = 0;
+    int myslot = 0;  // slot of the lane's bundle: parity * pool_max + index
     unsigned long long nsteps = 0, nbund = 0;
     Ray<R> r;
     ScatState<R> qs;
@@ -347,12 +347,11 @@ __global__ void __launch_bounds__(256, MINB) k_march(MarchArgs a) {
                         ws->ks[lane] = scatter_coef(S, e.nbg & 0xfffff, e.nbg >> 20);
                         ws->nev[lane] = 0u;
                     }
-                    myb = (e.kk >> 18) & 0x7ff;
-                    mypar = (e.kk >> 29) & 1;
+                    myslot = ((e.kk >> 29) & 1) * pool_max + ((e.kk >> 18) & 0x7ff);
                     took = true;
                     active = level_advance(r, S);
                     if (!active) {
-                        slots0[mypar * pool_max + myb] = r.De;
+                        slots0[myslot] = r.De;
                         fin = true;
                     }
                 }
@@ -361,7 +360,7 @@ __global__ void __launch_bounds__(256, MINB) k_march(MarchArgs a) {
             count -= navail;
             if (navail > 0) {
                 const unsigned tk = __ballot_sync(0xffffffffu, took);
-                const unsigned t1 = __ballot_sync(0xffffffffu, took && mypar == 1);
+                const unsigned t1 = __ballot_sync(0xffffffffu, took && myslot >= pool_max);
                 const unsigned fi = __ballot_sync(0xffffffffu, fin);
                 p1mask = (p1mask & ~tk) | t1;
                 amask = (amask | tk) & ~fi;
@@ -387,7 +386,7 @@ __global__ void __launch_bounds__(256, MINB) k_march(MarchArgs a) {
                     bool done = !(r.tra > r.tol);
                     if (!done && r.counter >= budget) done = !level_advance(r, S);
                     if (done) {
-                        slots0[mypar * pool_max + myb] = r.De;
+                        slots0[myslot] = r.De;
                         active = false;
                         fin = true;
                     }
@@ -413,6 +412,7 @@ __global__ void __launch_bounds__(256, MINB) k_march(MarchArgs a) {
         // ---- scattering: the new directions of every lane stopped at an event
         if constexpr (SCAT) {
             if (active && qs.dist < (R)0) {
+                const int mypar = myslot >= pool_max, myb = myslot - mypar * pool_max;
                 const ItemId it = decode_item(S, (mypar ? item0_1 : item0_0) + (myb >> lrpt));
                 uint4 c = scatter_counter(S.imax, S.jmax, it.kind, it.i, it.j, it.k, it.v, it.h0 + (myb & (rpt - 1)),
                                           ws->nev[lane]);

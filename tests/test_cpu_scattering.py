@@ -259,3 +259,59 @@ def test_energy_balance_closed_enclosure_with_scattering():
     var = (o["var64"] * vol ** 2).sum() + o["vw64"].sum() * area ** 2
     scale = (np.abs(o["q64"]) * vol).sum()
     assert abs(total) < 4.5 * np.sqrt(var) + 2e-3 * scale, (total, np.sqrt(var), scale)
+
+
+def test_phase_guide_brackets_return_the_bisection_index():
+    """The method of the device's angle search (restated here with numpy):
+    guide[q] = first a >= 1 with cdf[a] > q/G (nA-1 if none), then a
+    bisection over (guide[q] - 1, guide[q+1]] -- returns the index of a
+    bisection over the whole table, for every uniform including the bucket
+    edges q/G, the CDF values themselves and the largest float below 1, on
+    CDFs with flat stretches, jumps and long tails."""
+    from phase_tables import odd_phase_cdfs
+    G = 64
+    f32 = np.float32
+
+    def bisect_all(c, u):
+        lo, hi = 0, len(c) - 1
+        while hi - lo > 1:
+            mid = (lo + hi) >> 1
+            if u < c[mid]:
+                hi = mid
+            else:
+                lo = mid
+        return hi
+
+    def guided(c, guide, u):
+        q = min(int(f32(u) * f32(G)), G - 1)
+        lo, hi = int(guide[q]) - 1, int(guide[q + 1])
+        while hi - lo > 1:
+            mid = (lo + hi) >> 1
+            if u < c[mid]:
+                hi = mid
+            else:
+                lo = mid
+        return hi
+
+    for nA in (2, 3, 17, 91, 181):
+        if nA == 2:
+            cdfs = np.array([[0, 1]], np.float32)
+        elif nA == 3:
+            cdfs = np.array([[0, 0, 1], [0, 1, 1], [0, 0.5, 1]], np.float32)
+        else:
+            cdfs = odd_phase_cdfs(8, nA, nA)
+        for c in cdfs:
+            guide = []
+            a = 1
+            for q in range(G + 1):
+                thr = f32(q) / f32(G)
+                while a < nA - 1 and not (c[a] > thr):
+                    a += 1
+                guide.append(a)
+            us = [f32(0), f32(np.nextafter(f32(1), f32(0)))]
+            us += [f32(q) / f32(G) for q in range(G)]
+            us += [f32(np.nextafter(f32(q) / f32(G), f32(0))) for q in range(1, G)]
+            us += [x for x in c if x < 1] + [f32(np.nextafter(x, f32(0))) for x in c if 0 < x <= 1]
+            us += list(np.random.default_rng(nA).random(2000).astype(np.float32))
+            for u in us:
+                assert guided(c, guide, u) == bisect_all(c, u), (nA, u)

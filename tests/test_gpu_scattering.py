@@ -16,6 +16,8 @@ import pytest
 from radchan_b200 import api
 from radchan_b200 import workloads as W
 
+from phase_tables import odd_phase_cdfs
+
 pytestmark = pytest.mark.gpu
 
 
@@ -221,3 +223,31 @@ def test_batch_follows_a_member_changed_after_capture():
     for r, (scatter, rpt) in zip(results, ((False, rpt0), (True, rpt0), (True, 2 * rpt0))):
         a = alone(scatter, rpt)
         _equal(r, dict(q64=a.q64, var64=a.var64, qw64=a.qw64, vw64=a.vw64))
+
+
+def test_phase_cdf_with_flat_runs_and_jumps_equals_oracle():
+    """The device finds a scattering angle by a bracketed search of the
+    band's phase CDF (a guide per band); the oracle bisects the whole table.
+    On CDFs with flat stretches, jumps and long tails both pick the same
+    angle: traces and results agree bit for bit."""
+    O = _oracle()
+    p, tabs, _ = _nb_case(photmax=32)
+    nA = 91
+    theta = np.linspace(0.0, np.pi, nA)
+    rng = np.random.default_rng(4)
+    sc = api.Scattering.from_arrays(rng.uniform(1.0, 6.0, (24, 4)), theta, odd_phase_cdfs(24, nA, 5))
+    assert sc.validate() == ""
+    T = W.channel_field(p, seed=12)
+    s = api.Solver(p, tabs)
+    s.set_scattering(sc)
+    t = s.solve_async(T)
+    ids = [(k % 3, 1 + k % p.imax, 1 + (k // 3) % p.jmax, 1 + (k // 7) % p.kmax, k % p.nVar, k % p.photmax)
+           for k in range(300)]
+    g, gc = s.trace(t, ids, max_cells=128)
+    o, oc = O.trace(p, tabs, T, ids, max_cells=128, scatter=sc.arrays())
+    for a, b in zip(g, o):
+        assert (a.nb, a.g, a.nsteps, a.sx, a.sy, a.sz, a.tra) == (b.nb, b.g, b.nsteps, b.sx, b.sy, b.sz, b.tra)
+    np.testing.assert_array_equal(gc, oc)
+    r = s.collect(t)
+    _equal(r, O.solve(p, tabs, T, rpt=s.get_launch()[0], scatter=sc.arrays()))
+    s.close()
