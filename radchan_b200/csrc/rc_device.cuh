@@ -565,21 +565,25 @@ __device__ __forceinline__ uint4 scatter_counter(uint32_t imax, uint32_t jmax, i
     return make_uint4((uint32_t)h, (uint32_t)v | ((uint32_t)kind << 24), cell, nev);
 }
 
-// Free path to the first event of a bundle with counter words ctr and
-// scattering coefficient ks (draw 1; kNoEvent when ks = 0).
+// -ln(u) of draw 1 of a bundle with counter words ctr: its free path to the
+// first event in units of 1/k_s.  The draw does not depend on the band, so
+// the march takes it before the band is sampled (what is live at that
+// point is small).
 template <typename R>
-__device__ __forceinline__ R scatter_first_dist(const DSolve<R> &S, uint4 ctr, R ks) {
-    R dist = (R)kNoEvent;
-    if (ks > (R)0) {
-        rc_u32x4 c;
-        c.x = ctr.x;
-        c.y = ctr.y;
-        c.z = ctr.z;
-        c.w = 1u;
-        const rc_u32x4 d = rc_philox4x32_10(c, S.key0, S.key1);
-        dist = -RT<R>::log_((R)rc_u01(d.x)) / ks;
-    }
-    return dist;
+__device__ __forceinline__ R scatter_first_lnu(const DSolve<R> &S, uint4 ctr) {
+    rc_u32x4 c;
+    c.x = ctr.x;
+    c.y = ctr.y;
+    c.z = ctr.z;
+    c.w = 1u;
+    const rc_u32x4 d = rc_philox4x32_10(c, S.key0, S.key1);
+    return -RT<R>::log_((R)rc_u01(d.x));
+}
+
+// Free path to the first event: lnu / ks, kNoEvent when ks = 0.
+template <typename R>
+__device__ __forceinline__ R scatter_first_dist(R lnu, R ks) {
+    return (ks > (R)0) ? lnu / ks : (R)kNoEvent;
 }
 
 // Angle index of a uniform u on the phase CDF of a band: the first a in

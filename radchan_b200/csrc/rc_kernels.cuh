@@ -330,7 +330,7 @@ __global__ void k_trace(const DSolve<R> *Sp, int n, const rc_bundle_id *ids, rc_
         if (SCAT) {
             ctr = scatter_counter(S.imax, S.jmax, id.kind, id.i, id.j, id.k, id.v, id.h, 0u);
             ks = scatter_coef(S, e.nbg & 0xfffff, e.nbg >> 20);
-            qs.dist = scatter_first_dist(S, ctr, ks);
+            qs.dist = scatter_first_dist(ks > (R)0 ? scatter_first_lnu(S, ctr) : (R)0, ks);
         }
         bool active = level_advance(r, S);
         int ns = 0;

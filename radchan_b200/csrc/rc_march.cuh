@@ -291,12 +291,29 @@ __global__ void __launch_bounds__(256, MINB) k_march(MarchArgs a) {
                 const int h = it.h0 + (b & (rpt - 1));
                 if (it.kind >= 0 && h < S.photmax) {
                     nbund++;
+                    // with particles, draw 1 (scatter_first_lnu, written
+                    // out: the call form spilled) before the emission
+                    // itself: little is live then, so the variant fits the
+                    // register budget without spilling
+                    R lnu = (R)0;
+                    if constexpr (SCAT) {
+                        if (S.nA > 0) {
+                            const uint4 c0 = scatter_counter(S.imax, S.jmax, it.kind, it.i, it.j, it.k, it.v, h, 0u);
+                            rc_u32x4 c;
+                            c.x = c0.x;
+                            c.y = c0.y;
+                            c.z = c0.z;
+                            c.w = 1u;
+                            const rc_u32x4 d = rc_philox4x32_10(c, S.key0, S.key1);
+                            lnu = -RT<R>::log_((R)rc_u01(d.x));
+                        }
+                    }
                     ok = emit_bundle(e, S, it.kind, it.i, it.j, it.k, it.v, h);
                     e.kk |= (b << 18) | (epar << 29);
-                    if constexpr (SCAT)
-                        dist0 = scatter_first_dist(
-                            S, scatter_counter(S.imax, S.jmax, it.kind, it.i, it.j, it.k, it.v, h, 0u),
-                            scatter_coef(S, e.nbg & 0xfffff, e.nbg >> 20));
+                    if constexpr (SCAT) {
+                        const R ks = scatter_coef(S, e.nbg & 0xfffff, e.nbg >> 20);
+                        if (ks > (R)0) dist0 = lnu / ks;  // scatter_first_dist
+                    }
                 }
             }
             const unsigned m = __ballot_sync(0xffffffffu, ok);
