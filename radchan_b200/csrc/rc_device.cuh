@@ -40,6 +40,7 @@ constexpr int kWarp = 32;
 constexpr int kRing = 64;    // per-warp ring of emitted bundles (two waves)
 constexpr int kGuide = 256;  // buckets of the band-CDF guide tables
 constexpr int kFeedIdle = 14; // idle lanes that make a warp leave its step loop to take new bundles
+constexpr int kTurnGather = 5; // lanes waiting at scattering events that make a warp draw their turns
 constexpr int kChunkMax = 8;  // tiles a warp claims per work-queue fetch (guided: fewer near the end)
 constexpr int kPhaseGuide = 64;  // phase-CDF guide buckets per band (scattering turns)
 

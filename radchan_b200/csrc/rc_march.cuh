@@ -416,19 +416,29 @@ __global__ void __launch_bounds__(256, MINB) k_march(MarchArgs a) {
                     out0 -= __popc(fm) - n1;
                     amask &= ~fm;
                 }
-                // lanes stopped at a scattering event wait for the warp's next
-                // turn pass, which draws all their new directions at once
+                // lanes stopped at a scattering event wait for a turn pass,
+                // which draws all their new directions at once; the pass is
+                // long and runs on the waiting lanes only, so it waits until
+                // kTurnGather lanes wait, or every traced ray does
                 unsigned tm = 0u;
-                if constexpr (SCAT) tm = __ballot_sync(0xffffffffu, wait_turn);
+                bool turn_now = false;
+                if constexpr (SCAT) {
+                    tm = __ballot_sync(0xffffffffu, wait_turn);
+                    turn_now = __popc(tm) >= kTurnGather || (tm && !(amask & ~tm));
+                }
                 const int nidle = kWarp - __popc(amask & ~tm);
                 if (nidle == kWarp) break;
-                if (nidle >= kFeedIdle && (can_feed || tm)) break;
+                if (nidle >= kFeedIdle && (can_feed || turn_now)) break;
                 if (fm && ((((busy & emitted) & 1u) && out0 == 0) || (((busy & emitted) & 2u) && out1 == 0))) break;
             }
         }
-        // ---- scattering: the new directions of every lane stopped at an event
+        // ---- scattering: the new directions of every lane stopped at an
+        //      event, once kTurnGather lanes wait or no traced ray is left
+        //      that does not wait (waiting lanes never deadlock the warp)
         if constexpr (SCAT) {
-            if (active && qs.dist < (R)0) {
+            const unsigned tw = __ballot_sync(0xffffffffu, active && qs.dist < (R)0);
+            const bool turn_now = __popc(tw) >= kTurnGather || (tw && !(amask & ~tw));
+            if (turn_now && active && qs.dist < (R)0) {
                 const int mypar = myslot >= pool_max, myb = myslot - mypar * pool_max;
                 const ItemId it = decode_item(S, (mypar ? item0_1 : item0_0) + (myb >> lrpt));
                 uint4 c = scatter_counter(S.imax, S.jmax, it.kind, it.i, it.j, it.k, it.v, it.h0 + (myb & (rpt - 1)),
