@@ -54,14 +54,13 @@ def test_full_64_isothermal_source_vanishes():
 
 def test_full_64_energy_balance():
     """The volume integral of the source plus the net wall fluxes.  The
-    reciprocity estimate is conservative only up to its discretisation:
-    bundles leave every cell from its centre (kernel_fluid,
-    mc_gpu_noint.cu:117-122) and every wall cell from its centre point, so
+    estimator (the reference's) is not exactly conservative: bundles leave
+    every cell from its centre (kernel_fluid, mc_gpu_noint.cu:117-122), so
     in a non-uniform medium the exchange between two cells is not estimated
-    alike from either side.  On this channel that leaves about 1 % of the
-    integrated |source| (the oracle shows the same 2-3 % on small grids,
-    uniform or stretched), far below what a lost or double-counted term
-    would leave (each wall carries 60-70 % of it)."""
+    alike from either side, and long, nearly transparent paths add to it.
+    On this channel that leaves about 1 % of the integrated |source| (the
+    oracle shows 2-3 % on small grids), far below what a lost or
+    double-counted term would leave (each wall carries 60-70 % of it)."""
     p = _c2()
     tabs = W.tables_nb()
     s = api.Solver(p, tabs)
