@@ -641,8 +641,11 @@ void worker_loop(rc_server *sv) {
                         if (e) fail(sv, r, e, r->ctx ? r->ctx->err : g_err);
                     }
                     for (int k = 0; k < ns && forked; ++k) {
-                        cudaEventRecord(sv->join[k], sv->side[k]);
-                        cudaStreamWaitEvent(st, sv->join[k], 0);
+                        // a join that cannot be recorded is replaced by
+                        // waiting for the side stream on the host
+                        if (cudaEventRecord(sv->join[k], sv->side[k]) != cudaSuccess ||
+                            cudaStreamWaitEvent(st, sv->join[k], 0) != cudaSuccess)
+                            cudaStreamSynchronize(sv->side[k]);
                     }
                 }
                 for (SrvReq *r : sv->running)
