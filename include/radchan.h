@@ -13,7 +13,7 @@
  *
  * The reference configures everything at compile time (src/param/param.h,
  * src/param/NarrowBand.h) and reads its spectral tables from
- * properties/*.txt on every call (src/montecarlo/read_tables.cpp:21-96).
+ * the text files in properties/ on every call (src/montecarlo/read_tables.cpp:21-96).
  * Here the same parameter set is a runtime struct (rc_params), which can be
  * filled from an existing param.h / NarrowBand.h pair, and the tables are
  * uploaded once and stay resident on the device.

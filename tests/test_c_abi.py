@@ -25,6 +25,7 @@ def _build(tmp_path, name="legacy_abi"):
 def test_c_caller_compiles_and_links_against_the_library(tmp_path):
     assert os.path.exists(_build(tmp_path))
     assert os.path.exists(_build(tmp_path, "slab_abi"))
+    assert os.path.exists(_build(tmp_path, "slab_group"))
 
 
 @pytest.mark.gpu
@@ -57,3 +58,21 @@ def test_c_caller_slabs_over_ranks_equal_the_one_gpu_solve(tmp_path):
                        capture_output=True, text=True, timeout=600)
     assert r.returncode == 0, r.stdout + r.stderr
     assert "in 2 slabs: identical 1 nonzero 1" in r.stdout
+
+
+@pytest.mark.gpu
+def test_c_caller_slab_group_equals_the_plain_solve(tmp_path):
+    """One solve over a group of GPUs from C (tests/c/slab_group.c): the
+    group id, joining, rc_slab_solve on host arrays (the library's own
+    NCCL, field broadcast, in-place gathers) on a one-rank group equal the
+    plain solve of the same field bit for bit."""
+    exe = _build(tmp_path, "slab_group")
+    gold = os.path.join(HERE, "golden")
+    props = tmp_path / "properties"
+    props.mkdir()
+    r = subprocess.run([exe, os.path.join(gold, "param_channel64.h"), os.path.join(gold, "narrowband_channel64.h"),
+                        str(props)], capture_output=True, text=True, timeout=600,
+                       env=dict(os.environ, NCCL_NVLS_ENABLE="0"))
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert "identical 1 nonzero 1" in r.stdout
+
