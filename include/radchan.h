@@ -440,8 +440,9 @@ int rc_slab_comm_create(int device, int nranks, int rank, const void *id, double
  * the others' (their contents are overwritten).  q64/var64
  * [kmax][jmax][imax] (required) and qw64/vw64 [2][kmax][jmax] (optional)
  * receive the whole solution in the compact layouts of rc_collect on every
- * rank.  Each array may be device memory (used in place) or host memory
- * (staged through device buffers the communicator keeps).  Returns when
+ * rank.  Each array may be device memory of the communicator's GPU (used
+ * in place) or host memory (staged through device buffers the communicator
+ * keeps); device memory of another GPU is refused (RC_E_INVALID).  Returns when
  * the results are in place.  A solve error on one rank (RC_E_RANGE for a
  * non-finite field, which every rank sees) is returned after the
  * collectives, so the ranks stay in step; an argument error is returned

@@ -171,14 +171,18 @@ int ensure(rc_slab_comm *c, rc_slab_comm::Buf &b, size_t bytes, const char *what
     return RC_OK;
 }
 
-// Device memory (or managed memory) that NCCL and the solver can use as is.
-bool on_device(const void *ptr) {
+// Where an array lives: 1 device memory of `device` (or managed memory),
+// which NCCL and the solver use as is; 0 host memory (staged); -1 device
+// memory of another GPU (refused: it would be read across devices).
+int placement(const void *ptr, int device) {
     cudaPointerAttributes a;
     if (cudaPointerGetAttributes(&a, ptr) != cudaSuccess) {
         cudaGetLastError();  // a plain host pointer on an old runtime
-        return false;
+        return 0;
     }
-    return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+    if (a.type == cudaMemoryTypeManaged) return 1;
+    if (a.type == cudaMemoryTypeDevice) return a.device == device ? 1 : -1;
+    return 0;
 }
 
 Clock::time_point deadline_of(const rc_slab_comm *c) {
@@ -284,7 +288,9 @@ int rc_slab_solve(rc_slab_comm *c, rc_ctx *ctx, float *T, double *q64, double *v
     void *dv[5];
     bool staged[5];
     for (int a = 0; a < 5; ++a) {
-        staged[a] = user[a] && !on_device(user[a]);
+        const int where = user[a] ? placement(user[a], c->device) : 1;
+        if (where < 0) return fail(c, RC_E_INVALID, "an array lives on another GPU than the communicator's");
+        staged[a] = where == 0;
         dv[a] = user[a];
         if (staged[a]) {
             if ((rc = ensure(c, c->stage[a], bytes[a], "staging of a host array"))) return rc;
