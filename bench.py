@@ -67,7 +67,7 @@ BUNDLE_METRIC = "bundles/s & solves/s at 1% MC std, batched/served vs plain; ser
 # (dram__bytes_read.sum + dram__bytes_write.sum).  The march's working set
 # (temperature pyramid and tables, ~1.5 MB) is L2-resident, so the traffic
 # does not grow with photmax.
-K_MARCH_TRAFFIC = {"nb64": 990208 + 17664}
+K_MARCH_TRAFFIC = {"nb64": 1597184 + 0}
 
 
 def peaks():
